@@ -1,0 +1,165 @@
+// keq_common.cuh -- device utilities shared by the sm_100a kernels:
+// memory-ordering primitives, the bounded grid barrier of the persistent
+// kernels, NaN-aware max reductions and the warp reduce-scatter used for the
+// per-row velocity moments.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/keq_b200.h"
+
+namespace keq {
+
+constexpr int kLanes = 32;                 // velocities per tile (one warp width)
+constexpr double kTiny = 1.0e-300;         // clamp of n and T in the moment kernels
+constexpr double kInvSqrt2Pi = 0.39894228040143267794;  // 1/sqrt(2 pi), correctly rounded
+// Spin limit of every device-side wait (each poll sleeps ~64-256 ns): a few
+// seconds at most before the wait gives up and reports KEQ_ERR_TIMEOUT.
+constexpr unsigned long long kSpinLimit = 1ull << 25;
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ double ld_cg(const double* p) { return __ldcg(p); }
+
+// Non-negative doubles (and +NaN) order like their bit patterns, so the max
+// of a residual can be accumulated with an integer atomicMax.  NaN (0x7ff8..)
+// sorts above +Inf, i.e. a NaN residual wins, as torch.max propagates NaN.
+__device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
+    atomicMax(reinterpret_cast<unsigned long long*>(addr),
+              static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
+__device__ __forceinline__ double nan_max(double a, double b) {
+    if (a != a || b != b) return __longlong_as_double(0x7ff8000000000000ll);
+    return a > b ? a : b;
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = nan_max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Grid barrier for a cooperative launch.  One arrival per CTA; the last
+// arriving CTA releases the generation word.  Every wait is bounded: on
+// timeout the CTA records KEQ_ERR_TIMEOUT in *err and the caller leaves its
+// loop.  The acquire load also invalidates the SM's L1, so ordinary loads
+// after the barrier observe other CTAs' stores made before it.
+struct GridBarrier {
+    unsigned count;
+    unsigned gen;
+};
+
+__device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned nblocks, int* err) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned g = ld_acquire(&gb->gen);
+        __threadfence();
+        const unsigned prev = atomicAdd(&gb->count, 1u);
+        if (prev == nblocks - 1) {
+            gb->count = 0u;
+            __threadfence();
+            st_release(&gb->gen, g + 1u);
+        } else {
+            unsigned long long it = 0;
+            unsigned ns = 32;
+            while (ld_acquire(&gb->gen) == g) {
+                if (++it > kSpinLimit) {
+                    atomicOr(err, 1 << KEQ_ERR_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(ns);
+                if (ns < 256) ns <<= 1;
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Spin (bounded) until *flag >= want.  Returns false on timeout.
+__device__ __forceinline__ bool wait_flag_geq(const unsigned* flag, unsigned want, int* err) {
+    unsigned long long it = 0;
+    unsigned ns = 16;
+    while (ld_acquire(flag) < want) {
+        if (++it > kSpinLimit) {
+            atomicOr(err, 1 << KEQ_ERR_TIMEOUT);
+            return false;
+        }
+        __nanosleep(ns);
+        if (ns < 128) ns <<= 1;
+    }
+    return true;
+}
+
+// Warp reduce-scatter of ROWS x Q partial sums held by every lane
+// (acc[r*Q + q]).  On return lanes holding row r (see owner_row()) carry the
+// warp-wide sums of that row in acc[0..Q-1].  The combination order is fixed
+// (butterfly on lane bits 4..0), so results are reproducible.
+//   ROWS must be a power of two <= 32.
+template <int ROWS, int Q>
+__device__ __forceinline__ void warp_reduce_scatter(double (&acc)[ROWS * Q], int lane) {
+    // Level lvl uses lane bit (16 >> lvl).  While more than one row is left
+    // the row set is halved; afterwards the remaining bits all-reduce.
+#pragma unroll
+    for (int lvl = 0; lvl < 5; ++lvl) {
+        const int bit = 16 >> lvl;
+        const int nrows = (ROWS >> lvl) > 0 ? (ROWS >> lvl) : 1;
+        if (nrows > 1) {
+            const int half = nrows >> 1;
+            const bool upper = (lane & bit) != 0;
+#pragma unroll
+            for (int r = 0; r < half; ++r) {
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    const double lo = acc[r * Q + q];
+                    const double hi = acc[(r + half) * Q + q];
+                    const double mine = upper ? hi : lo;
+                    const double send = upper ? lo : hi;
+                    acc[r * Q + q] = mine + __shfl_xor_sync(0xffffffffu, send, bit);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], bit);
+        }
+    }
+}
+
+// Row owned by `lane` after warp_reduce_scatter<ROWS,Q>: lane bit 4 is the
+// most significant bit of the row index, then bit 3, ...
+template <int ROWS>
+__device__ __forceinline__ int owner_row(int lane) {
+    int row = 0;
+#pragma unroll
+    for (int lvl = 0; lvl < 5; ++lvl) {
+        const int nrows = (ROWS >> lvl) > 0 ? (ROWS >> lvl) : 1;
+        if (nrows > 1 && (lane & (16 >> lvl))) row += nrows >> 1;
+    }
+    return row;
+}
+
+// True for the single lane that writes row owner_row(lane): the lane bits
+// not used for the row id are zero.
+template <int ROWS>
+__device__ __forceinline__ bool owner_writes(int lane) {
+    int lvls = 0;
+#pragma unroll
+    for (int n = ROWS; n > 1; n >>= 1) ++lvls;
+    const int low_mask = (1 << (5 - lvls)) - 1;
+    return (lane & low_mask) == 0;
+}
+
+}  // namespace keq

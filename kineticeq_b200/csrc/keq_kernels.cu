@@ -1,0 +1,270 @@
+// keq_kernels.cu -- kernel-level drop-ins of the reference's extension
+// modules (implicit_fused, gtsv, lo_blocktridiag) behind the C ABI.  The
+// fused time-step kernels (keq_implicit.cu, keq_holo.cu) do not call these;
+// they serve callers that use the reference's module-level API directly.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "keq_common.cuh"
+#include "keq_internal.h"
+
+namespace keq {
+
+// ---- K1: velocity moments, one warp per row -------------------------------
+// implicit_kernels.cu:28-81 semantics (clamps), reduction = per-lane strided
+// partial sums + fixed butterfly.
+__global__ void __launch_bounds__(256) moments_kernel(const double* __restrict__ f,
+                                                      const double* __restrict__ v, int nx,
+                                                      int nv, double dv, double* __restrict__ n,
+                                                      double* __restrict__ nu,
+                                                      double* __restrict__ T) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= nx) return;
+    const double* row = f + (size_t)warp * nv;
+    double p0 = 0.0, p1 = 0.0, p2 = 0.0;
+    for (int j = lane; j < nv; j += 32) {
+        const double x = row[j], vj = v[j];
+        p0 += x;
+        p1 += x * vj;
+        p2 += x * vj * vj;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        p0 += __shfl_xor_sync(0xffffffffu, p0, o);
+        p1 += __shfl_xor_sync(0xffffffffu, p1, o);
+        p2 += __shfl_xor_sync(0xffffffffu, p2, o);
+    }
+    if (lane == 0) {
+        const double n_raw = p0 * dv, nu_raw = p1 * dv, s2 = p2 * dv;
+        const double nn = n_raw > kTiny ? n_raw : kTiny;
+        const double u = nu_raw / nn;
+        double Tg = s2 / nn - u * u;
+        if (!(Tg > 0.0)) Tg = kTiny;
+        n[warp] = nn;
+        nu[warp] = nu_raw;
+        T[warp] = Tg;
+    }
+}
+
+// ---- K2: Maxwellian + upwind implicit assembly ----------------------------
+// implicit_kernels.cu:84-134; one thread per (v_j, k), k fastest.
+__global__ void __launch_bounds__(256) build_system_kernel(
+    const double* __restrict__ B0, const double* __restrict__ v, const double* __restrict__ n,
+    const double* __restrict__ nu, const double* __restrict__ Tg, const double* __restrict__ fl,
+    const double* __restrict__ fr, int nx, int nv, double dt, double dx, double tau_tilde,
+    double inv_sqrt_2pi, double* __restrict__ dl, double* __restrict__ dd,
+    double* __restrict__ du, double* __restrict__ B) {
+    const int n_inner = nx - 2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n_inner * nv) return;
+    const int j = (int)(t / n_inner), k = (int)(t % n_inner);
+    const double vj = v[j];
+    const double alpha = vj > 0.0 ? (dt / dx) * vj : 0.0;
+    const double beta = vj < 0.0 ? (dt / dx) * (-vj) : 0.0;
+    const int i = k + 1;
+    const double ni = n[i] > kTiny ? n[i] : kTiny;
+    const double Ti = Tg[i] > kTiny ? Tg[i] : kTiny;
+    const double ui = nu[i] / ni;
+    const double inv_tau = (ni * sqrt(Ti)) / tau_tilde;
+    dd[t] = 1.0 + alpha + beta + dt * inv_tau;
+    dl[t] = k == 0 ? 0.0 : -alpha;
+    du[t] = k == n_inner - 1 ? 0.0 : -beta;
+    const double diff = vj - ui;
+    const double fM = ni * inv_sqrt_2pi / sqrt(Ti) * exp(-0.5 * diff * diff / Ti);
+    double rhs = B0[t] + dt * inv_tau * fM;
+    if (k == 0) rhs += alpha * fl[j];
+    if (k == n_inner - 1) rhs += beta * fr[j];
+    B[t] = rhs;
+}
+
+// ---- K3: batched general tridiagonal solve ---------------------------------
+// Thomas without pivoting, pivot floor +-1e-300 (the CPU twin's semantics,
+// cpu_kernel/BGK1D1V/gtsv_cpu/gtsv_binding.cpp:32-37, 51-97); one thread per
+// system, modified super-diagonal kept in the workspace (d is not modified).
+__global__ void __launch_bounds__(128) gtsv_kernel(const double* __restrict__ dl,
+                                                   const double* __restrict__ d,
+                                                   const double* __restrict__ du,
+                                                   double* __restrict__ B, int n, int batch,
+                                                   double* __restrict__ cp) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= batch) return;
+    const size_t o = (size_t)b * n;
+    auto piv = [](double x) {
+        if (fabs(x) >= 1.0e-300) return x;
+        return x < 0.0 ? -1.0e-300 : 1.0e-300;
+    };
+    // forward elimination exactly as the CPU twin: d'_i = d_i - w du_{i-1}
+    double dprev = d[o];
+    cp[o] = dprev;
+    for (int i = 1; i < n; ++i) {
+        const double w = dl[o + i] / piv(dprev);
+        const double di = d[o + i] - w * du[o + i - 1];
+        B[o + i] -= w * B[o + i - 1];
+        cp[o + i] = di;
+        dprev = di;
+    }
+    B[o + n - 1] /= piv(cp[o + n - 1]);
+    for (int i = n - 1; i-- > 0;) B[o + i] = (B[o + i] - du[o + i] * B[o + i + 1]) / piv(cp[o + i]);
+}
+
+// ---- K5: batched 3x3 block-tridiagonal solve -------------------------------
+__device__ __forceinline__ void m3mul(const double* A, const double* B, double* C) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            C[3 * i + j] = A[3 * i] * B[j] + A[3 * i + 1] * B[3 + j] + A[3 * i + 2] * B[6 + j];
+}
+__device__ __forceinline__ void m3vec(const double* A, const double* x, double* y) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) y[i] = A[3 * i] * x[0] + A[3 * i + 1] * x[1] + A[3 * i + 2] * x[2];
+}
+// Adjugate inverse; |det| < 1e-30 -> zero matrix
+// (lo_blocktridiag/block_tridiag_kernel.cu:32-68, 248-250 convention).
+__device__ __forceinline__ void m3inv(const double* M, double* Mi) {
+    const double a00 = M[0], a01 = M[1], a02 = M[2], a10 = M[3], a11 = M[4], a12 = M[5],
+                 a20 = M[6], a21 = M[7], a22 = M[8];
+    const double c00 = (a11 * a22 - a12 * a21), c01 = -(a10 * a22 - a12 * a20),
+                 c02 = (a10 * a21 - a11 * a20);
+    const double c10 = -(a01 * a22 - a02 * a21), c11 = (a00 * a22 - a02 * a20),
+                 c12 = -(a00 * a21 - a01 * a20);
+    const double c20 = (a01 * a12 - a02 * a11), c21 = -(a00 * a12 - a02 * a10),
+                 c22 = (a00 * a11 - a01 * a10);
+    const double det = a00 * c00 + a01 * c01 + a02 * c02;
+    if (!(fabs(det) >= 1e-30)) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Mi[k] = 0.0;
+        return;
+    }
+    const double id = 1.0 / det;
+    Mi[0] = c00 * id; Mi[1] = c10 * id; Mi[2] = c20 * id;
+    Mi[3] = c01 * id; Mi[4] = c11 * id; Mi[5] = c21 * id;
+    Mi[6] = c02 * id; Mi[7] = c12 * id; Mi[8] = c22 * id;
+}
+
+// Block Thomas, one thread per system; C' and D' in the workspace.
+__global__ void __launch_bounds__(64) block_thomas_kernel(const double* __restrict__ A,
+                                                          const double* __restrict__ Bm,
+                                                          const double* __restrict__ C,
+                                                          const double* __restrict__ D,
+                                                          double* __restrict__ X, int n, int batch,
+                                                          double* __restrict__ ws) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= batch) return;
+    const size_t mo = (size_t)b * n * 9, vo = (size_t)b * n * 3;
+    double* Cp = ws + (size_t)b * n * 12;
+    double* Dp = Cp + (size_t)n * 9;
+    double Mi[9], T9[9], t3[3], M[9], rhs[3];
+    for (int i = 0; i < n; ++i) {
+        if (i == 0) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) M[k] = Bm[mo + k];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) rhs[k] = D[vo + k];
+        } else {
+            m3mul(A + mo + 9 * (size_t)i, Cp + 9 * (size_t)(i - 1), T9);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) M[k] = Bm[mo + 9 * (size_t)i + k] - T9[k];
+            m3vec(A + mo + 9 * (size_t)i, Dp + 3 * (size_t)(i - 1), t3);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) rhs[k] = D[vo + 3 * (size_t)i + k] - t3[k];
+        }
+        m3inv(M, Mi);
+        if (i < n - 1) m3mul(Mi, C + mo + 9 * (size_t)i, Cp + 9 * (size_t)i);
+        m3vec(Mi, rhs, Dp + 3 * (size_t)i);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) X[vo + 3 * (size_t)(n - 1) + k] = Dp[3 * (size_t)(n - 1) + k];
+    for (int i = n - 2; i >= 0; --i) {
+        m3vec(Cp + 9 * (size_t)i, X + vo + 3 * (size_t)(i + 1), t3);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) X[vo + 3 * (size_t)i + k] = Dp[3 * (size_t)i + k] - t3[k];
+    }
+}
+
+}  // namespace keq
+
+namespace {
+keq_status launch_status() {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        keq_internal_set_cuda_error(e);
+        return KEQ_ERR_CUDA;
+    }
+    return KEQ_OK;
+}
+}  // namespace
+
+extern "C" {
+
+keq_status keq_moments_n_nu_T(const double* f, const double* v, int32_t nx, int32_t nv, double dv,
+                              double* n, double* nu, double* T, keq_stream_t stream) {
+    if (!f || !v || !n || !nu || !T || nx < 1 || nv < 1) return KEQ_ERR_INVALID;
+    const long long threads = (long long)nx * 32;
+    const int blocks = (int)((threads + 255) / 256);
+    keq::moments_kernel<<<blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(f, v, nx, nv,
+                                                                                   dv, n, nu, T);
+    return launch_status();
+}
+
+keq_status keq_build_system_from_moments(const double* B0, const double* v, int32_t nx,
+                                         int32_t nv, double dt, double dx, double tau_tilde,
+                                         double inv_sqrt_2pi, const double* n, const double* nu,
+                                         const double* T, const double* f_bc_l,
+                                         const double* f_bc_r, double* dl, double* dd,
+                                         double* du, double* B, keq_stream_t stream) {
+    if (!B0 || !v || !n || !nu || !T || !f_bc_l || !f_bc_r || !dl || !dd || !du || !B)
+        return KEQ_ERR_INVALID;
+    if (nx < 3 || nv < 1) return KEQ_ERR_INVALID;
+    const long long total = (long long)(nx - 2) * nv;
+    const int blocks = (int)((total + 255) / 256);
+    keq::build_system_kernel<<<blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        B0, v, n, nu, T, f_bc_l, f_bc_r, nx, nv, dt, dx, tau_tilde, inv_sqrt_2pi, dl, dd, du, B);
+    return launch_status();
+}
+
+keq_status keq_gtsv_workspace_size(int32_t n, int32_t batch, size_t* bytes) {
+    if (!bytes || n < 0 || batch < 0) return KEQ_ERR_INVALID;
+    *bytes = sizeof(double) * (size_t)(n > 0 ? n : 1) * (size_t)(batch > 0 ? batch : 1);
+    return KEQ_OK;
+}
+
+keq_status keq_gtsv_strided_inplace(const double* dl, const double* d, const double* du,
+                                    double* B, int32_t n, int32_t batch, void* workspace,
+                                    size_t workspace_bytes, keq_stream_t stream) {
+    if (n < 0 || batch < 0) return KEQ_ERR_INVALID;
+    if (n == 0 || batch == 0) return KEQ_OK;
+    if (!dl || !d || !du || !B || !workspace) return KEQ_ERR_INVALID;
+    size_t need = 0;
+    keq_gtsv_workspace_size(n, batch, &need);
+    if (workspace_bytes < need || reinterpret_cast<uintptr_t>(workspace) % 8)
+        return KEQ_ERR_WORKSPACE;
+    keq::gtsv_kernel<<<(batch + 127) / 128, 128, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        dl, d, du, B, n, batch, static_cast<double*>(workspace));
+    return launch_status();
+}
+
+keq_status keq_block_tridiag_workspace_size(int32_t n, int32_t batch, size_t* bytes) {
+    if (!bytes || n < 0 || batch < 0) return KEQ_ERR_INVALID;
+    *bytes = sizeof(double) * 12 * (size_t)(n > 0 ? n : 1) * (size_t)(batch > 0 ? batch : 1);
+    return KEQ_OK;
+}
+
+keq_status keq_block_tridiag_solve(const double* A, const double* B, const double* C,
+                                   const double* D, double* X, int32_t n, int32_t batch,
+                                   void* workspace, size_t workspace_bytes,
+                                   keq_stream_t stream) {
+    if (n < 0 || batch < 0) return KEQ_ERR_INVALID;
+    if (n == 0 || batch == 0) return KEQ_OK;
+    if (!A || !B || !C || !D || !X || !workspace) return KEQ_ERR_INVALID;
+    size_t need = 0;
+    keq_block_tridiag_workspace_size(n, batch, &need);
+    if (workspace_bytes < need || reinterpret_cast<uintptr_t>(workspace) % 8)
+        return KEQ_ERR_WORKSPACE;
+    keq::block_thomas_kernel<<<(batch + 63) / 64, 64, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        A, B, C, D, X, n, batch, static_cast<double*>(workspace));
+    return launch_status();
+}
+
+}  // extern "C"

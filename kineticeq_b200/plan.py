@@ -1,0 +1,178 @@
+"""Host-side plans over the C ABI: a list of independent BGK1D1V instances
+stepped together by the persistent kernel (one launch per time step for the
+whole list).
+
+Each instance owns two state buffers ``a`` and ``b`` (nx, nv) FP64 on the
+device; the state ping-pongs between them without copies and
+``ImplicitPlan.state(i)`` returns the buffer that holds the newest state.
+All device memory is torch-allocated; the library only receives pointers.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+from typing import Sequence
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+_STATS_DTYPE = np.dtype([
+    ("status", "<i4"), ("iters", "<i4"), ("aa_applied", "<i4"), ("lo_iters", "<i4"),
+    ("residual", "<f8"), ("std_residual", "<f8"), ("lo_residual", "<f8"),
+    ("std_lo_residual", "<f8"), ("max_YI", "<f8"), ("total_iters", "<i8"),
+    ("total_steps", "<i8")])
+assert _STATS_DTYPE.itemsize == N.STATS_BYTES
+
+
+def implicit_params_struct(sp=None, fixed_iters: int = 0, **kw) -> N.ImplicitParams:
+    """implicit.Params (or keywords) -> keq_implicit_params; the clamps of
+    bgk1d_implicit_cuda_kernel.py:49-65 are applied inside the library."""
+    g = (lambda k, d: kw[k] if k in kw else getattr(sp, k, d))
+    conv = str(g("conv_type", "f")).lower()
+    if conv not in ("f", "w"):
+        raise ValueError(f"invalid conv_type={conv!r}, expected 'f' or 'w'")
+    return N.ImplicitParams(
+        int(g("picard_iter", 16)), float(g("picard_tol", 1e-4)), float(g("abs_tol", 1e-16)),
+        1 if conv == "w" else 0, int(bool(g("aa_enable", False))), int(g("aa_m", 6)),
+        float(g("aa_beta", 1.0)), int(g("aa_stride", 1)), int(g("aa_start_iter", 2)),
+        float(g("aa_reg", 1e-10)), float(g("aa_alpha_max", 50.0)), int(fixed_iters))
+
+
+@dataclass
+class InstanceSpec:
+    """One solve: grid (nx, nv, dx, dv, v on the device), dt, tau_tilde and
+    the two (nx, nv) FP64 device buffers; ``a`` holds f^n on entry."""
+    v: torch.Tensor
+    dx: float
+    dv: float
+    dt: float
+    tau_tilde: float
+    a: torch.Tensor
+    b: torch.Tensor
+
+    @property
+    def nx(self) -> int:
+        return int(self.a.shape[0])
+
+    @property
+    def nv(self) -> int:
+        return int(self.a.shape[1])
+
+
+def _check_buf(t: torch.Tensor, name: str) -> None:
+    if not t.is_cuda:
+        raise RuntimeError(f"{name} must be a CUDA tensor")
+    if t.dtype != torch.float64:
+        raise RuntimeError(f"{name} must be float64")
+    if not t.is_contiguous():
+        raise RuntimeError(f"{name} must be contiguous")
+
+
+class LazyStats:
+    """Device-resident keq_step_stats records, copied to the host only when
+    read (one synchronisation per read, none per step)."""
+
+    def __init__(self, dev: torch.Tensor, n: int):
+        self._dev = dev
+        self._n = n
+
+    def fetch(self) -> np.ndarray:
+        raw = np.ascontiguousarray(self._dev.cpu().numpy()).reshape(-1)
+        return raw.view(_STATS_DTYPE)[: self._n].copy()
+
+
+class ImplicitPlan:
+    """Batched implicit Picard stepping of independent instances."""
+
+    def __init__(self, specs: Sequence[InstanceSpec], params, stream=None):
+        lib = N.load()
+        if len(specs) == 0:
+            raise ValueError("empty instance list")
+        plist = list(params) if isinstance(params, (list, tuple)) else [params]
+        if len(plist) not in (1, len(specs)):
+            raise ValueError("params: one record or one per instance")
+        pstructs = [p if isinstance(p, N.ImplicitParams) else implicit_params_struct(p)
+                    for p in plist]
+        self.device = specs[0].a.device
+        self.specs = list(specs)
+        self.n = len(specs)
+        self._stream = stream
+        sh = N.stream_handle(stream)
+        self.stats_dev = torch.zeros((self.n, N.STATS_BYTES), dtype=torch.uint8,
+                                     device=self.device)
+        self._ws = []
+        inst = (N.Instance * self.n)()
+        for i, s in enumerate(self.specs):
+            _check_buf(s.a, "f")
+            _check_buf(s.b, "f_tmp")
+            _check_buf(s.v, "v")
+            if s.a.shape != s.b.shape or s.a.dim() != 2 or s.v.numel() != s.a.shape[1]:
+                raise RuntimeError("f / f_tmp must be (nx, nv) and v must be (nv,)")
+            p = pstructs[i if len(pstructs) > 1 else 0]
+            grid = N.Grid(s.nx, s.nv, float(s.dx), float(s.dv), s.v.data_ptr())
+            nbytes = C.c_size_t(0)
+            N.check(lib.keq_implicit_instance_workspace_size(C.byref(grid), C.byref(p),
+                                                             C.byref(nbytes)), "workspace query")
+            ws = torch.empty((max(int(nbytes.value), 256),), dtype=torch.uint8,
+                             device=self.device)
+            self._ws.append(ws)
+            inst[i] = N.Instance(grid, float(s.dt), float(s.tau_tilde), s.a.data_ptr(),
+                                 s.b.data_ptr(), self.stats_dev[i].data_ptr(), ws.data_ptr())
+        parr = (N.ImplicitParams * len(pstructs))(*pstructs)
+        per = 1 if len(pstructs) > 1 else 0
+        nbytes = C.c_size_t(0)
+        N.check(lib.keq_implicit_plan_workspace_size(inst, self.n, parr, per, C.byref(nbytes)),
+                "plan workspace query")
+        self._plan_ws = torch.empty((max(int(nbytes.value), 256),), dtype=torch.uint8,
+                                    device=self.device)
+        handle = C.c_void_p(0)
+        N.check(lib.keq_implicit_plan_create(inst, self.n, parr, per,
+                                             self._plan_ws.data_ptr(), self._plan_ws.numel(),
+                                             sh, C.byref(handle)), "plan creation")
+        self._h = handle
+        self._lib = lib
+        self.parity = 0  # 0: newest state in `a`, 1: in `b`
+        self.stats = LazyStats(self.stats_dev, self.n)
+
+    def step(self, n_steps: int = 1) -> None:
+        N.check(self._lib.keq_plan_step(self._h, int(n_steps), int(self.parity),
+                                        N.stream_handle(self._stream)), "implicit step")
+        self.parity = (self.parity + int(n_steps)) & 1
+
+    def state(self, i: int) -> torch.Tensor:
+        s = self.specs[i]
+        return s.a if self.parity == 0 else s.b
+
+    def other(self, i: int) -> torch.Tensor:
+        s = self.specs[i]
+        return s.b if self.parity == 0 else s.a
+
+    def device_error_bits(self) -> int:
+        v = C.c_int32(0)
+        N.check(self._lib.keq_plan_error(self._h, N.stream_handle(self._stream), C.byref(v)),
+                "plan error query")
+        return int(v.value)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.keq_plan_destroy(self._h)
+            self._h = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def grid_of(nx: int, nv: int, Lx: float = 1.0, v_max: float = 10.0, device="cuda"):
+    """(v on device, dx, dv) exactly as core/states/state_1d.py:30-58."""
+    v = torch.linspace(-v_max, v_max, nv, dtype=torch.float64).to(device)
+    return v, float(Lx / (nx - 1)), float((2.0 * v_max) / (nv - 1))
+
+
+def _inv_sqrt_2pi() -> float:
+    return 1.0 / math.sqrt(2.0 * math.pi)
