@@ -1,0 +1,376 @@
+"""Throughput benchmark of the B200 BGK1D1V implicit time step.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+               [--workload NAME] [--no-cpu-baseline] [--no-e2e]
+
+Metric: cell-velocity updates/s = sum over instances of nx*nv*steps / seconds
+(one update = one (x_i, v_k) entry advanced one full time step, whatever the
+number of Picard iterations).  Default workload: the large plain FP64 case,
+4096 x 512 cells, v in [-10, 10], dt = 1e-5, tau_tilde = 5e-5, Sod initial
+state, Picard tolerance 1e-10 (cap 64), Anderson depth m = 5 (200 steps =
+the case's T_total).
+
+ours:      K time steps, each ONE launch of the persistent step kernel, timed
+           with CUDA events on the launching stream; L2 is flushed (256 MiB
+           write) before every step outside the timed window.  e2e repeats the
+           measurement through the C ABI with host buffers: pinned f^n -> device,
+           step, f^{n+1} -> pinned host, all inside the timed window.
+reference: the CPU oracle (C restatement of the reference's cpu_kernel path,
+           all host threads) on the same workload, a bounded number of steps.
+Multi-GPU (torchrun): every rank steps its own replica (independent
+instances, no collective on the data path); value = all ranks' updates /
+max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    # name: (nx, nv, dt, tau_tilde, implicit params, steps of the case)
+    "implicit-4096x512-aa5-tau5e-5": (4096, 512, 1e-5, 5e-5,
+                                      dict(picard_iter=64, picard_tol=1e-10, abs_tol=1e-16,
+                                           aa_enable=True, aa_m=5), 200),
+    "implicit-4096x512-tau5e-5": (4096, 512, 1e-5, 5e-5,
+                                  dict(picard_iter=64, picard_tol=1e-10, abs_tol=1e-16), 200),
+    "implicit-4096x512-aa5-tau5e-3": (4096, 512, 1e-5, 5e-3,
+                                      dict(picard_iter=64, picard_tol=1e-10, abs_tol=1e-16,
+                                           aa_enable=True, aa_m=5), 200),
+    "implicit-256x128-tau5e-5": (256, 128, 5e-6, 5e-5,
+                                 dict(picard_iter=64, picard_tol=1e-10, abs_tol=1e-16), 100),
+    "implicit-8192x1024-aa5-tau1e-4": (8192, 1024, 1e-5, 1e-4,
+                                       dict(picard_iter=64, picard_tol=1e-10, abs_tol=1e-16,
+                                            aa_enable=True, aa_m=5), 200),
+}
+DEFAULT_WORKLOAD = "implicit-4096x512-aa5-tau5e-5"
+METRIC = "cell-velocity updates/s"
+BYTES_PER_CELL_ITER = 24  # read f^n, read f^(m), write f^(m+1) (FP64)
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic_from_profiles(workload: str):
+    """Per-launch DRAM bytes recorded by the committed ncu summary, scaled to
+    this workload (profiles/*.md lines 'traffic_bytes_per_cell_iter: X')."""
+    for p in sorted((ROOT / "profiles").glob("*.md")):
+        for line in p.read_text().splitlines():
+            if line.startswith("traffic_bytes_per_cell_iter:"):
+                try:
+                    return float(line.split(":", 1)[1].strip().split()[0]), p.name
+                except ValueError:
+                    pass
+    return None, None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(f"/tmp/keq_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() in ("active", "1", "yes"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        return dist, dist.get_rank(), ws
+    return None, 0, 1
+
+
+def _max_over_ranks(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def make_instance(name: str):
+    import torch
+
+    from kineticeq_b200.plan import ImplicitPlan, InstanceSpec, implicit_params_struct
+    from kineticeq_b200.schemes.common import maxwellian
+    from kineticeq_b200.state import allocate_state_1d1v
+
+    nx, nv, dt, tau, sp, _ = WORKLOADS[name]
+    st = allocate_state_1d1v(nx, nv, 1.0, 10.0, "cuda", torch.float64)
+    # Sod initial state (BGK1D1V_params.py:26-30 defaults)
+    x = st.x
+    st.n = torch.where(x < 0.5, 1.0, 0.125).to(torch.float64)
+    st.u = torch.zeros_like(x)
+    st.T = torch.where(x < 0.5, 1.0, 0.8).to(torch.float64)
+    st.f.copy_(maxwellian(st))
+    spec = InstanceSpec(v=st.v, dx=st.dx, dv=st.dv, dt=dt, tau_tilde=tau, a=st.f,
+                        b=torch.empty_like(st.f))
+    plan = ImplicitPlan([spec], implicit_params_struct(**sp))
+    return plan, st
+
+
+def run_ours(args, dist, rank, world):
+    import torch
+
+    from kineticeq_b200 import _native as N
+
+    name = args.workload
+    nx, nv, dt, tau, sp, case_steps = WORKLOADS[name]
+    plan, st = make_instance(name)
+    f0 = st.f.clone()
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    for _ in range(args.warmup):
+        plan.step(1)
+    torch.cuda.synchronize()
+    # restart from the initial state so the timed steps are the case's first K
+    plan.state(0).copy_(f0)
+    iters0 = int(plan.stats.fetch()[0]["total_iters"])
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    launches = 0
+    _barrier(dist)
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            starts[k].record(stream)
+            plan.step(1)
+            launches += 1
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+    _barrier(dist)
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    rec = plan.stats.fetch()[0]
+    if int(rec["status"]) != 0:
+        raise RuntimeError(f"device status {N.status_text(int(rec['status']))}")
+    iters = int(rec["total_iters"]) - iters0
+    ms_max = _max_over_ranks(dist, ms)
+    cells = nx * nv
+    value = world * cells * args.steps / (ms_max / 1e3)
+
+    # e2e through the C ABI with host buffers (pinned), copies inside the timing
+    e2e = None
+    if not args.no_e2e:
+        host_in = f0.cpu().pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        e_s = torch.cuda.Event(enable_timing=True)
+        e_e = torch.cuda.Event(enable_timing=True)
+        ksteps = args.steps
+        _barrier(dist)
+        torch.cuda.synchronize()
+        e_s.record(stream)
+        src = host_in
+        for k in range(ksteps):
+            plan.state(0).copy_(src, non_blocking=True)
+            plan.step(1)
+            host_out.copy_(plan.state(0), non_blocking=True)
+            src = host_out
+        e_e.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = _max_over_ranks(dist, e_s.elapsed_time(e_e))
+        nb = host_in.numel() * host_in.element_size()
+        e2e = {"value": world * cells * ksteps / (e2e_ms / 1e3), "unit": METRIC,
+               "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb}
+
+    # roofline of the step kernel (one launch per step)
+    peak, peak_kind = _peaks()
+    bytes_per_launch = BYTES_PER_CELL_ITER * cells * (iters / args.steps)
+    achieved = bytes_per_launch / (ms / args.steps / 1e3) / 1e9
+    tpc, tsrc = _traffic_from_profiles(name)
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+            "traffic": (round(tpc * cells * iters / args.steps) if tpc else None),
+            "traffic_source": tsrc, "bytes_per_launch_algorithmic": round(bytes_per_launch),
+            "kernel": "keq::implicit_step_kernel"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(name, f0.cpu().numpy(), st, budget_s=args.cpu_seconds)
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": round(value, 1), "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 5),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (Sod initial state, generated on the device)",
+            "config": {"workload": name, "nx": nx, "nv": nv, "dt": dt, "tau_tilde": tau,
+                       "picard_tol": sp["picard_tol"], "picard_iter": sp["picard_iter"],
+                       "anderson_m": sp.get("aa_m") if sp.get("aa_enable") else 0,
+                       "instances_per_gpu": 1, "parallelism": f"replicas x{world}",
+                       "l2": "flushed (256 MiB write) before every timed step",
+                       "mean_picard_iters_per_step": round(iters / args.steps, 3)},
+            "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(out))
+
+
+def cpu_baseline(name, f0, st, budget_s=20.0):
+    """The oracle (C restatement of the reference's cpu_kernel path) on the
+    host cores: as many time steps of the same workload as fit the budget."""
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    from oracle import oracle as O
+
+    nx, nv, dt, tau, sp, _ = WORKLOADS[name]
+    v = st.v.cpu().numpy()
+    p = O.implicit_params(None, **sp)
+    f = f0.copy()
+    O.lib()
+    t0 = time.perf_counter()
+    steps = iters = 0
+    while True:
+        bl = O.implicit_step(f, v, st.dx, st.dv, dt, tau, p)
+        steps += 1
+        iters += bl["picard_iter"]
+        el = time.perf_counter() - t0
+        if el >= budget_s or steps >= 200:
+            break
+    val = nx * nv * steps / el
+    return {"value": round(val, 1), "unit": METRIC, "cores": int(os.environ["OMP_NUM_THREADS"]),
+            "kind": "port", "sample": f"first {steps} time steps of {name} ({iters} Picard "
+                                      f"iterations) in {el:.1f} s"}
+
+
+def run_reference(args, dist, rank, world):
+    """--impl reference: the reference's CPU implementation of the path (its
+    C restatement; the reference itself does not travel) on the host cores."""
+    if rank != 0:
+        return
+    import torch
+
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle import oracle as O
+
+    name = args.workload
+    nx, nv, dt, tau, sp, _ = WORKLOADS[name]
+    g = O.Grid(nx, nv)
+    v = g.v()
+    f = O.initial_condition(g)
+    p = O.implicit_params(None, **sp)
+    # bounded sample: at most ~budget seconds of timed steps
+    for _ in range(min(args.warmup, 1)):
+        O.implicit_step(f.copy(), v, g.dx, g.dv, dt, tau, p)
+    t0 = time.perf_counter()
+    steps = iters = 0
+    while steps < args.steps:
+        bl = O.implicit_step(f, v, g.dx, g.dv, dt, tau, p)
+        steps += 1
+        iters += bl["picard_iter"]
+        if time.perf_counter() - t0 > args.cpu_seconds * 6:
+            break
+    el = time.perf_counter() - t0
+    val = nx * nv * steps / el
+    sample = f"first {steps} time steps of {name} ({iters} Picard iterations), {el:.1f} s"
+    out = {"impl": "reference", "metric": METRIC, "value": round(val, 1), "unit": METRIC,
+           "n_gpus": world, "steps": steps, "warmup": min(args.warmup, 1),
+           "ms_per_step": round(el * 1e3 / steps, 3), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (Sod)",
+           "config": {"workload": name, "nx": nx, "nv": nv, "dt": dt, "tau_tilde": tau},
+           "cpu_baseline": {"value": round(val, 1), "unit": METRIC, "cores": threads,
+                            "kind": "port", "sample": sample},
+           "e2e": {"value": round(val, 1), "unit": METRIC, "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0},
+           "torch_threads": torch.get_num_threads()}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    dist, rank, world = _dist()
+    try:
+        if args.impl == "reference":
+            run_reference(args, dist, rank, world)
+        else:
+            run_ours(args, dist, rank, world)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

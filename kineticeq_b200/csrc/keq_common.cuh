@@ -41,6 +41,55 @@ __device__ __forceinline__ double nan_max(double a, double b) {
     return a > b ? a : b;
 }
 
+// 1/d by Newton-Raphson iteration r <- r + r (1 - d r) (quadratic
+// convergence) from a single-precision seed: the seed's relative error is
+// below 2^-22, two steps bring it below 2^-80, so the result is within one
+// rounding of 1/d.  Valid for 2^-120 < |d| < 2^120; outside that range the
+// IEEE division is used.
+__device__ __forceinline__ double recip_nr(double d) {
+    const double ad = fabs(d);
+    if (!(ad > 7.5e-37 && ad < 1.3e36)) return 1.0 / d;
+    double r = (double)__frcp_rn((float)d);
+    double e = fma(-d, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-d, r, 1.0);
+    return fma(r, e, r);
+}
+
+// Running maximum of ratios num/den without a division per element: the
+// maximum is kept as a fraction and compared by cross-multiplication
+// (num_a * den_b > num_b * den_a for positive finite denominators).
+// Elements with a zero, infinite or NaN denominator or numerator take an
+// exact slow path (IEEE division, NaN-propagating max), so the result equals
+// max_i(num_i / den_i) as torch.max computes it, up to one rounding.
+struct FracMax {
+    double num, den, special;
+    __device__ __forceinline__ FracMax() : num(0.0), den(1.0), special(0.0) {}
+    __device__ __forceinline__ void add(double a, double b) {
+        if (b > 0.0 && b < 1.0e300 && a >= 0.0 && a < 1.0e300) {
+            if (a * den > num * b) {
+                num = a;
+                den = b;
+            }
+        } else {
+            const double q = a / b;
+            special = (q != q || special != special) ? q + special : (q > special ? q : special);
+        }
+    }
+    __device__ __forceinline__ double value() const {
+        const double q = num / den;
+        if (special != special) return special;
+        return q > special ? q : special;
+    }
+};
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = nan_max(v, __shfl_xor_sync(0xffffffffu, v, o));

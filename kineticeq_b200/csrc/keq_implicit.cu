@@ -47,11 +47,10 @@
 
 namespace keq {
 
-constexpr int kWarps = 8;
+constexpr int kWarps = 8;                // warps per CTA
 constexpr int kThreads = kWarps * 32;
-constexpr int kRows = 8;                 // scan positions per thread
-constexpr int kLX = kWarps * kRows;      // scan positions per tile (64)
-constexpr int kRB = kThreads;            // rows per reduction block
+constexpr int kR = 16;                   // scan positions (rows) per warp-tile
+constexpr int kRW = 32;                  // rows per reduction warp unit
 constexpr int kMaxAACols = 8;            // Anderson ring columns (aa_m <= 7)
 constexpr int kMaxPairs = kMaxAACols * (kMaxAACols + 1) / 2;
 constexpr int kPartQ = 4;                // doubles per (v-tile,row) partial
@@ -73,7 +72,7 @@ struct ImpInst {
     double* W;       // 3*nx  : n | nu | T   (W^(m))
     double* Wn;      // 3*nx  : moments of the newest iterate (unfloored)
     double* Wc;      // 4*nx  : per-row (u, -1/(2T), n/sqrt(2 pi T), dt/tau)
-    double* Wb;      // 8     : moments of the two boundary rows (n,nu,T) x2 + flags
+    double* Wb;      // 8     : moments of the two boundary rows
     double* part;    // nvt*n_inner*kPartQ
     double* lb;      // nvt*nchunks*3*32  (P | Y | X per lane)
     unsigned* lbflag;// nvt*nchunks
@@ -98,27 +97,31 @@ struct PlanDev {
     ImpInst* inst;
     long long* tile_off;  // n_inst+1
     long long* rb_off;    // n_inst+1
-    unsigned* tickets;    // max_iter+1
+    unsigned* tickets;    // max_iter+1 (reserved)
 };
 
-struct SMem {
-    double segP[kWarps][32];
-    double segY[kWarps][32];
-    double carry[kWarps][32];
-    double red[kWarps][4];
-    double alpha[kMaxAACols];
-    long long tile;
-    int flags;
+// Per-warp shared memory: the instance descriptor of the warp's current work
+// item, the f^n tile / local solution, the local propagator and the row
+// coefficients.
+struct WarpSmem {
+    ImpInst I;
+    double fy[kR][32];     // f^n of the warp-tile, then the local solution y
+    double fP[kR][32];     // local propagator P (x = y + P * carry)
+    double coef[kR][4];    // (u, -1/(2T), n/sqrt(2 pi T), dt/tau) per row
+    int cur_b;
+    int pad;
 };
 
 __device__ __forceinline__ int find_inst(const long long* off, int n, long long t) {
     int lo = 0, hi = n;  // off[lo] <= t < off[hi]
     while (hi - lo > 1) {
         const int mid = (lo + hi) >> 1;
-        if (off[mid] <= t) lo = mid; else hi = mid;
+        if (__ldg(&off[mid]) <= t) lo = mid; else hi = mid;
     }
     return lo;
 }
+
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
 __device__ __forceinline__ bool iter_done(const ImpInst& I, int m) {
     // Convergence test of iteration m (bgk1d_implicit_cuda_kernel.py:241).
@@ -134,19 +137,28 @@ __device__ __forceinline__ bool inst_active(const ImpInst& I, int m) {
     return !iter_done(I, m - 1);
 }
 
+// Anderson call z (after Picard iteration z) applies the combination iff
+// z+1 >= start, (z+1-start) % stride == 0 and its history length
+// min(z+1, cols) >= 2 (bgk1d_implicit_cuda_kernel.py:247-282, bgk1d_aa_cpu.py:131).
+__device__ __forceinline__ bool aa_applies(const ImpInst& I, int z) {
+    const int mh = (z + 1) < I.aa_cols ? (z + 1) : I.aa_cols;
+    return I.aa_on && (z + 1) >= I.aa_start && ((z + 1 - I.aa_start) % I.aa_stride == 0) &&
+           mh >= 2;
+}
+
 // Per-row solve coefficients from (n, nu, T): implicit_kernels.cu:115-125
 // (n, T clamped at 1e-300; 1/tau = n sqrt(T)/tau_tilde).
-__device__ __forceinline__ void row_coeffs(const ImpInst& I, double n, double nu, double T,
-                                           double* c4) {
+__device__ __forceinline__ void row_coeffs(double tau_tilde, double dt, double n, double nu,
+                                           double T, double* c4) {
     const double ni = n > kTiny ? n : kTiny;
     const double Ti = T > kTiny ? T : kTiny;
     const double ui = nu / ni;
     const double sT = sqrt(Ti);
-    const double inv_tau = (ni * sT) / I.tau_tilde;
+    const double inv_tau = (ni * sT) / tau_tilde;
     c4[0] = ui;
     c4[1] = -0.5 / Ti;
     c4[2] = ni * kInvSqrt2Pi / sT;
-    c4[3] = I.dt * inv_tau;
+    c4[3] = dt * inv_tau;
 }
 
 // C1/K1 moment semantics from raw sums.
@@ -168,6 +180,42 @@ __device__ __forceinline__ double clamp_min_t(double x, double lo) {
     return (x != x || x >= lo) ? x : lo;
 }
 
+// Sum of the per-v-tile partial moments of interior row k, in v-tile order
+// (loads issued in batches of 8 so their latencies overlap).
+__device__ __forceinline__ void sum_partials(const double* part, int nvt, int n_inner, int k,
+                                             double* s0, double* s1, double* s2) {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int v0 = 0; v0 < nvt; v0 += 8) {
+        double2 p01[8];
+        double p2[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            if (v0 + q < nvt) {
+                const double* p = part + ((size_t)(v0 + q) * n_inner + k) * kPartQ;
+                p01[q] = __ldcg(reinterpret_cast<const double2*>(p));
+                p2[q] = __ldcg(p + 2);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            if (v0 + q < nvt) {
+                a0 += p01[q].x;
+                a1 += p01[q].y;
+                a2 += p2[q];
+            }
+        }
+    }
+    *s0 = a0;
+    *s1 = a1;
+    *s2 = a2;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 // ---- tile geometry --------------------------------------------------------
 struct TileGeo {
     bool pos;      // velocities > 0 -> forward scan
@@ -181,34 +229,36 @@ __device__ __forceinline__ TileGeo tile_geo(const ImpInst& I, int vt, int c, int
     g.pos = vt >= I.nt_neg;
     g.j = g.pos ? I.kp + 32 * (vt - I.nt_neg) + lane : I.kp - 32 * (vt + 1) + lane;
     g.lane_ok = g.pos ? (g.j < I.nv) : (g.j >= 0);
-    g.s0 = c * kLX;
+    g.s0 = c * kR;
     return g;
 }
 
-__device__ __forceinline__ int scan_row(const ImpInst& I, bool pos, int s) {
-    return pos ? 1 + s : I.nx - 2 - s;
+__device__ __forceinline__ int scan_row(int nx, bool pos, int s) { return pos ? 1 + s : nx - 2 - s; }
+
+// Copy an instance descriptor into the warp's shared memory.  Reads of the
+// descriptor then cannot alias the warp's global stores.
+__device__ __forceinline__ void stage_warp(WarpSmem& w, const ImpInst* src, int b) {
+    if (w.cur_b != b) {
+        __syncwarp();
+        const int lane = threadIdx.x & 31;
+        const int* s = reinterpret_cast<const int*>(src);
+        int* d = reinterpret_cast<int*>(&w.I);
+        for (int q = lane; q < (int)(sizeof(ImpInst) / sizeof(int)); q += 32) d[q] = __ldg(s + q);
+        __syncwarp();
+        if (lane == 0) w.cur_b = b;
+    }
+    __syncwarp();
 }
 
-// ---- P1: partial moments of f^n -----------------------------------------
-__device__ void moments_tile(const ImpInst& I, int vt, int c, const double* __restrict__ f) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const TileGeo g = tile_geo(I, vt, c, lane);
-    const double vj = g.lane_ok ? I.v[g.j] : 0.0;
-    double acc[kRows * 3];
-#pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-        const int s = g.s0 + warp * kRows + r;
-        double x = 0.0;
-        if (s < I.n_inner && g.lane_ok) x = f[(size_t)scan_row(I, g.pos, s) * I.nv + g.j];
-        acc[3 * r + 0] = x;
-        acc[3 * r + 1] = x * vj;
-        acc[3 * r + 2] = x * vj * vj;
-    }
-    warp_reduce_scatter<kRows, 3>(acc, lane);
-    if (owner_writes<kRows>(lane)) {
-        const int s = g.s0 + warp * kRows + owner_row<kRows>(lane);
+// Warp reduce-scatter of the 3 moments of kR rows held per lane, in two
+// halves of kR/2 rows, and store of the per-(v-tile,row) partials.
+__device__ __forceinline__ void store_partials(const ImpInst& I, const TileGeo& g, int vt, int lane,
+                                               double (&acc)[kR / 2 * 3], int half) {
+    warp_reduce_scatter<kR / 2, 3>(acc, lane);
+    if (owner_writes<kR / 2>(lane)) {
+        const int s = g.s0 + half * (kR / 2) + owner_row<kR / 2>(lane);
         if (s < I.n_inner) {
-            const int k = scan_row(I, g.pos, s) - 1;
+            const int k = scan_row(I.nx, g.pos, s) - 1;
             double* p = I.part + ((size_t)vt * I.n_inner + k) * kPartQ;
             p[0] = acc[0];
             p[1] = acc[1];
@@ -217,195 +267,213 @@ __device__ void moments_tile(const ImpInst& I, int vt, int c, const double* __re
     }
 }
 
-// ---- S(m): fused solve tile --------------------------------------------------
-__device__ void solve_tile(int* err, const ImpInst& I, int vt, int c, int m, SMem& sm,
-                           const double* __restrict__ fn, double* __restrict__ fo) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// ---- P1: partial moments of f^n (one warp-tile) -------------------------
+__device__ void moments_wtile(const ImpInst& I, int vt, int c, const double* __restrict__ f) {
+    const int lane = threadIdx.x & 31;
     const TileGeo g = tile_geo(I, vt, c, lane);
-    const double vj = g.lane_ok ? I.v[g.j] : 0.0;
-    const double cpl = I.dtdx * fabs(vj);     // alpha (v>0) or beta (v<0)
-    const double one_plus = 1.0 + cpl;          // 1 + alpha + beta
-    const size_t tile_id = (size_t)c * I.nvt + vt;
+    const double vj = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        double acc[kR / 2 * 3];
+#pragma unroll
+        for (int r = 0; r < kR / 2; ++r) {
+            const int s = g.s0 + h * (kR / 2) + r;
+            double x = 0.0;
+            if (s < I.n_inner && g.lane_ok) x = f[(size_t)scan_row(I.nx, g.pos, s) * I.nv + g.j];
+            acc[3 * r + 0] = x;
+            acc[3 * r + 1] = x * vj;
+            acc[3 * r + 2] = x * vj * vj;
+        }
+        store_partials(I, g, vt, lane, acc, h);
+    }
+}
+
+// ---- S(m): fused solve of one warp-tile (32 velocities x kR rows) --------
+__device__ void solve_wtile(int* err, WarpSmem& w, int vt, int c, int m,
+                            const double* __restrict__ fn, double* __restrict__ fo, FracMax& q1,
+                            FracMax& q2, bool& bad) {
+    const ImpInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const TileGeo g = tile_geo(I, vt, c, lane);
+    const int nx = I.nx, nv = I.nv, n_inner = I.n_inner, nvt = I.nvt;
+    const size_t tile_id = (size_t)c * nvt + vt;
     const unsigned f_agg = 2u * (unsigned)m + 1u, f_inc = 2u * (unsigned)m + 2u;
 
-    // Anderson-combined W^(m) for this tile's rows (iterations after an
-    // applied Anderson step).  alpha was solved by the last block of R(m-1).
-    // Anderson call m-1 applied iff (m >= start, (m-start) % stride == 0) and
-    // its history length min(m, cols) >= 2 (bgk1d_implicit_cuda_kernel.py:248-251).
-    const int mh = m < I.aa_cols ? m : I.aa_cols;
-    const bool aa_apply_prev = I.aa_on && m >= 1 && m >= I.aa_start &&
-                               ((m - I.aa_start) % I.aa_stride == 0) && mh >= 2;
-
-    double y[kRows], Pm[kRows], fold[kRows];
-    double Pseg = 1.0, Yseg = 0.0;
+    // 1. f^n tile -> shared memory (asynchronous copy); the previous iterate
+    //    -> registers (this warp wrote it in the previous iteration: tiles are
+    //    statically assigned); the boundary carry.
+    double fold[kR];
 #pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-        const int s = g.s0 + warp * kRows + r;
-        y[r] = Yseg;
-        Pm[r] = Pseg;
+    for (int r = 0; r < kR; ++r) {
+        const int s = g.s0 + r;
         fold[r] = 0.0;
-        if (s < I.n_inner) {
-            const int i = scan_row(I, g.pos, s);
-            double c4[4];
-            if (aa_apply_prev) {
-                // bgk1d_aa_cpu.py:170-188 on the fly for row i.
-                const int k = i - 1, d = 3 * I.n_inner;
+        if (s < n_inner && g.lane_ok) {
+            const size_t idx = (size_t)scan_row(nx, g.pos, s) * nv + g.j;
+            cp_async8(&w.fy[r][lane], fn + idx);
+            if (m > 0) fold[r] = fo[idx];
+        }
+    }
+    cp_async_commit();
+    const double vj = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
+    const double Xb = (c == 0 && g.lane_ok) ? fn[(size_t)(g.pos ? 0 : nx - 1) * nv + g.j] : 0.0;
+
+    // 2. row coefficients of W^(m) (lane r handles row r).  After an applied
+    //    Anderson call the combination w = beta G alpha + (1-beta) w_new,
+    //    floors and |u| <= u_max (bgk1d_aa_cpu.py:170-188) is formed here
+    //    from the history ring.
+    if (lane < kR) {
+        const int s = g.s0 + lane;
+        double c4[4] = {0.0, 0.0, 0.0, 0.0};
+        if (s < n_inner) {
+            const int i = scan_row(nx, g.pos, s);
+            if (m >= 1 && aa_applies(I, m - 1)) {
+                const int k = i - 1, d = 3 * n_inner;
+                const int mh = m < I.aa_cols ? m : I.aa_cols;
                 const int head_out = m % I.aa_cols;
-                double w[3];
+                double al[kMaxAACols];
+                int col[kMaxAACols];
+#pragma unroll
+                for (int jj = 0; jj < kMaxAACols; ++jj) {
+                    al[jj] = jj < mh ? ld_cg(&I.alpha[(size_t)(m - 1) * kMaxAACols + jj]) : 0.0;
+                    col[jj] = ((head_out - mh + jj) % I.aa_cols + I.aa_cols) % I.aa_cols;
+                }
+                double wv[3];
 #pragma unroll
                 for (int q = 0; q < 3; ++q) {
+                    double gv[kMaxAACols];
+#pragma unroll
+                    for (int jj = 0; jj < kMaxAACols; ++jj)
+                        gv[jj] = jj < mh ? ld_cg(&I.aaG[(size_t)col[jj] * d + q * n_inner + k]) : 0.0;
                     double acc = 0.0;
-                    for (int jj = 0; jj < mh; ++jj) {
-                        const int col = ((head_out - mh + jj) % I.aa_cols + I.aa_cols) % I.aa_cols;
-                        acc += ld_cg(&I.aaG[(size_t)col * d + q * I.n_inner + k]) * sm.alpha[jj];
-                    }
-                    const double wnew = ld_cg(&I.Wn[q * I.nx + i]);
-                    w[q] = acc * I.aa_beta + (1.0 - I.aa_beta) * wnew;
+#pragma unroll
+                    for (int jj = 0; jj < kMaxAACols; ++jj)
+                        if (jj < mh) acc += gv[jj] * al[jj];
+                    const double wnew = ld_cg(&I.Wn[q * nx + i]);
+                    wv[q] = acc * I.aa_beta + (1.0 - I.aa_beta) * wnew;
                 }
-                const double nm = clamp_min_t(w[0], 1e-12);
-                const double Tm = clamp_min_t(w[2], 1e-12);
-                double um = w[1] / nm;
+                const double nm = clamp_min_t(wv[0], 1e-12);
+                const double Tm = clamp_min_t(wv[2], 1e-12);
+                double um = wv[1] / nm;
                 if (!isfinite(um)) um = 0.0;
                 um = um < -I.u_max ? -I.u_max : (um > I.u_max ? I.u_max : um);
                 const double num = nm * um;
-                row_coeffs(I, nm, num, Tm, c4);
-                if (vt == 0 && lane == 0) {
+                row_coeffs(I.tau_tilde, I.dt, nm, num, Tm, c4);
+                if (vt == 0) {
                     I.W[i] = nm;
-                    I.W[I.nx + i] = num;
-                    I.W[2 * I.nx + i] = Tm;
+                    I.W[nx + i] = num;
+                    I.W[2 * nx + i] = Tm;
                 }
             } else {
                 const double2 c01 = __ldcg(reinterpret_cast<const double2*>(&I.Wc[4 * (size_t)i]));
                 const double2 c23 = __ldcg(reinterpret_cast<const double2*>(&I.Wc[4 * (size_t)i + 2]));
                 c4[0] = c01.x; c4[1] = c01.y; c4[2] = c23.x; c4[3] = c23.y;
             }
-            if (g.lane_ok) {
-                const size_t idx = (size_t)i * I.nv + g.j;
-                const double fin = fn[idx];
-                fold[r] = (m == 0) ? fin : fo[idx];
-                const double diff = vj - c4[0];
-                const double M = c4[2] * exp(diff * diff * c4[1]);
-                const double b = fma(c4[3], M, fin);
-                const double dd = one_plus + c4[3];
-                const double rr = __drcp_rn(dd);
-                Yseg = fma(cpl, Yseg, b) * rr;
-                Pseg = Pseg * (cpl * rr);
-                y[r] = Yseg;
-                Pm[r] = Pseg;
-            }
         }
-    }
-    sm.segP[warp][lane] = Pseg;
-    sm.segY[warp][lane] = Yseg;
-    __syncthreads();
-
-    if (warp == 0) {
-        // tile aggregate (nested composition of the 8 segment maps)
-        double Pt = 1.0, Yt = 0.0;
 #pragma unroll
-        for (int w = 0; w < kWarps; ++w) {
-            Yt = fma(sm.segP[w][lane], Yt, sm.segY[w][lane]);
-            Pt = sm.segP[w][lane] * Pt;
-        }
-        double* lbt = I.lb + tile_id * 96;
-        lbt[lane] = Pt;
-        lbt[32 + lane] = Yt;
-        __threadfence();
-        __syncwarp();
-        if (lane == 0) st_release(&I.lbflag[tile_id], f_agg);
+        for (int q = 0; q < 4; ++q) w.coef[lane][q] = c4[q];
+    }
+    cp_async_wait_all();
+    __syncwarp();
 
-        // carry into the tile
-        double X;
-        if (c == 0) {
-            X = g.lane_ok ? fn[(size_t)(g.pos ? 0 : I.nx - 1) * I.nv + g.j] : 0.0;
-        } else {
-            int k0 = -1;  // nearest predecessor chunk with an inclusive value
-            bool ok = true;
-            for (int base = c - 1; base >= 0 && ok; base -= 32) {
-                const int kk = base - lane;
-                unsigned fl = f_inc;  // chunks < 0: the boundary acts as inclusive
-                if (kk >= 0) {
-                    const unsigned* fp = &I.lbflag[(size_t)kk * I.nvt + vt];
-                    if (!wait_flag_geq(fp, f_agg, err)) ok = false;
-                    fl = ld_acquire(fp);
-                }
-                const unsigned incl = __ballot_sync(0xffffffffu, fl >= f_inc);
-                if (!__all_sync(0xffffffffu, ok)) { ok = false; break; }
-                if (incl) {
-                    const int l = __ffs(incl) - 1;
-                    k0 = base - l;
-                    break;
-                }
-            }
-            if (!ok) {
-                X = 0.0;
-            } else {
-                if (k0 < 0)
-                    X = g.lane_ok ? fn[(size_t)(g.pos ? 0 : I.nx - 1) * I.nv + g.j] : 0.0;
-                else
-                    X = ld_cg(&I.lb[((size_t)k0 * I.nvt + vt) * 96 + 64 + lane]);
-                for (int k = (k0 < 0 ? 0 : k0 + 1); k < c; ++k) {
-                    const double* q = I.lb + ((size_t)k * I.nvt + vt) * 96;
-                    X = fma(ld_cg(q + lane), X, ld_cg(q + 32 + lane));
-                }
-            }
+    // 3. Maxwellian + assembly + local solve; y and P to shared memory
+    const double cpl = I.dtdx * fabs(vj);  // alpha (v>0) or beta (v<0)
+    const double one_plus = 1.0 + cpl;     // 1 + alpha + beta
+    double Pseg = 1.0, Yseg = 0.0;
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+        const int s = g.s0 + r;
+        if (s < n_inner && g.lane_ok) {
+            const double fin = w.fy[r][lane];
+            if (m == 0) fold[r] = fin;
+            const double u = w.coef[r][0], nh = w.coef[r][1];
+            const double cm = w.coef[r][2], dti = w.coef[r][3];
+            const double diff = vj - u;
+            const double M = cm * exp(diff * diff * nh);
+            const double b = fma(dti, M, fin);
+            const double rr = recip_nr(one_plus + dti);
+            Yseg = fma(cpl, Yseg, b) * rr;
+            Pseg = Pseg * (cpl * rr);
         }
-        lbt[64 + lane] = fma(Pt, X, Yt);
-        __threadfence();
+        w.fy[r][lane] = Yseg;
+        w.fP[r][lane] = Pseg;
+    }
+
+    // 4. publish the tile map, decoupled look-back, publish the inclusive carry
+    double* lbt = I.lb + tile_id * 96;
+    double X = Xb;
+    if (c == 0) {
+        lbt[64 + lane] = fma(Pseg, X, Yseg);
+        fence_acq_rel();
         __syncwarp();
         if (lane == 0) st_release(&I.lbflag[tile_id], f_inc);
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) {
-            sm.carry[w][lane] = X;
-            X = fma(sm.segP[w][lane], X, sm.segY[w][lane]);
+    } else {
+        lbt[lane] = Pseg;
+        lbt[32 + lane] = Yseg;
+        fence_acq_rel();
+        __syncwarp();
+        if (lane == 0) st_release(&I.lbflag[tile_id], f_agg);
+        int k0 = -1;  // nearest predecessor chunk with an inclusive value
+        bool ok = true;
+        for (int base = c - 1; base >= 0; base -= 32) {
+            const int kk = base - lane;
+            unsigned fl = f_inc;  // chunks < 0: the boundary acts as inclusive
+            if (kk >= 0) {
+                const unsigned* fp = &I.lbflag[(size_t)kk * nvt + vt];
+                if (!wait_flag_geq(fp, f_agg, err)) ok = false;
+                fl = ld_acquire(fp);
+            }
+            if (!__all_sync(0xffffffffu, ok)) { ok = false; break; }
+            const unsigned incl = __ballot_sync(0xffffffffu, fl >= f_inc);
+            if (incl) {
+                k0 = base - (__ffs(incl) - 1);
+                break;
+            }
         }
+        if (!ok) {
+            X = 0.0;
+        } else {
+            X = k0 >= 0 ? ld_cg(&I.lb[((size_t)k0 * nvt + vt) * 96 + 64 + lane])
+                        : (g.lane_ok ? fn[(size_t)(g.pos ? 0 : nx - 1) * nv + g.j] : 0.0);
+            for (int k = k0 + 1; k < c; ++k) {
+                const double* q = I.lb + ((size_t)k * nvt + vt) * 96;
+                X = fma(ld_cg(q + lane), X, ld_cg(q + 32 + lane));
+            }
+        }
+        lbt[64 + lane] = fma(Pseg, X, Yseg);
+        fence_acq_rel();
+        __syncwarp();
+        if (lane == 0) st_release(&I.lbflag[tile_id], f_inc);
     }
-    __syncthreads();
 
-    // final values, residual, non-finite check, partial moments
-    const double Xc = sm.carry[warp][lane];
-    double acc[kRows * 3];
-    double q1 = 0.0, q2 = 0.0;
-    bool bad = false;
+    // 5. final values, residual (bgk1d_conv_util.py:25-33), non-finite
+    //    check, partial moments
+    const double tol = I.tol, abs_tol = I.abs_tol;
 #pragma unroll
-    for (int r = 0; r < kRows; ++r) {
-        const int s = g.s0 + warp * kRows + r;
-        double x = 0.0;
-        if (s < I.n_inner && g.lane_ok) {
-            const int i = scan_row(I, g.pos, s);
-            x = fma(Pm[r], Xc, y[r]);
-            fo[(size_t)i * I.nv + g.j] = x;
-            const double df = fabs(x - fold[r]);
-            const double ref = nan_max(fabs(x), fabs(fold[r]));
-            q1 = nan_max(q1, df / (I.abs_tol + I.tol * ref));
-            const double rc = (ref != ref || ref >= I.abs_tol) ? ref : I.abs_tol;
-            q2 = nan_max(q2, df / rc);
-            bad |= !isfinite(x);
+    for (int h = 0; h < 2; ++h) {
+        double acc[kR / 2 * 3];
+#pragma unroll
+        for (int rr = 0; rr < kR / 2; ++rr) {
+            const int r = h * (kR / 2) + rr;
+            const int s = g.s0 + r;
+            double x = 0.0;
+            if (s < n_inner && g.lane_ok) {
+                const int i = scan_row(nx, g.pos, s);
+                x = fma(w.fP[r][lane], X, w.fy[r][lane]);
+                fo[(size_t)i * nv + g.j] = x;
+                const double o = fold[r];
+                const double df = fabs(x - o);
+                const double ref = nan_max(fabs(x), fabs(o));
+                q1.add(df, abs_tol + tol * ref);
+                q2.add(df, (ref != ref || ref >= abs_tol) ? ref : abs_tol);
+                bad |= !isfinite(x);
+            }
+            acc[3 * rr + 0] = x;
+            acc[3 * rr + 1] = x * vj;
+            acc[3 * rr + 2] = x * vj * vj;
         }
-        acc[3 * r + 0] = x;
-        acc[3 * r + 1] = x * vj;
-        acc[3 * r + 2] = x * vj * vj;
+        store_partials(I, g, vt, lane, acc, h);
     }
-    warp_reduce_scatter<kRows, 3>(acc, lane);
-    if (owner_writes<kRows>(lane)) {
-        const int s = g.s0 + warp * kRows + owner_row<kRows>(lane);
-        if (s < I.n_inner) {
-            const int k = scan_row(I, g.pos, s) - 1;
-            double* p = I.part + ((size_t)vt * I.n_inner + k) * kPartQ;
-            p[0] = acc[0];
-            p[1] = acc[1];
-            p[2] = acc[2];
-        }
-    }
-    if (I.conv_type == 0) {
-        q1 = warp_max(q1);
-        q2 = warp_max(q2);
-        if (lane == 0) {
-            atomic_max_nonneg(&I.res[2 * m], q1);
-            atomic_max_nonneg(&I.res[2 * m + 1], q2);
-        }
-    }
-    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&I.nonfin[m], 1);
+    __syncwarp();
 }
 
 // ---- Anderson: small symmetric solve (Cholesky, min-norm fall-back) -------
@@ -488,151 +556,147 @@ __device__ __noinline__ void aa_small_solve(int m, double* A, double* x) {
     }
 }
 
-// Block-wide sum of one value per thread into red[] (fixed order); result
-// valid in thread 0.
-__device__ __forceinline__ double block_sum(double v, SMem& sm, int slot) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) sm.red[warp][slot] = v;
-    __syncthreads();
-    double t = 0.0;
-    if (threadIdx.x == 0)
-        for (int w = 0; w < kWarps; ++w) t += sm.red[w][slot];
-    __syncthreads();
-    return t;
+// Last reduction unit of Anderson call m: Gram matrix from the per-unit
+// partials (lane L sums units L, L+32, ...; fixed butterfly across lanes),
+// regularised Cholesky solve, normalisation by the sum, clip
+// (bgk1d_aa_cpu.py:146-168).
+__device__ __noinline__ void aa_finalize(const double* gpart, int nrb, int mh, double reg,
+                                         double alpha_max, double* alpha_out) {
+    const int lane = threadIdx.x & 31;
+    double A[kMaxAACols * kMaxAACols];
+    int pj = 0;
+    for (int p = 0; p < mh; ++p)
+        for (int q = p; q < mh; ++q, ++pj) {
+            double part_sum = 0.0;
+            for (int r2 = lane; r2 < nrb; r2 += 32) part_sum += ld_cg(&gpart[(size_t)r2 * kMaxPairs + pj]);
+            const double sv = warp_sum(part_sum);
+            A[p * mh + q] = sv;
+            A[q * mh + p] = sv;
+        }
+    if (lane == 0) {
+        for (int p = 0; p < mh; ++p) A[p * mh + p] += reg;
+        double al[kMaxAACols];
+        aa_small_solve(mh, A, al);
+        double asum = 0.0;
+        for (int p = 0; p < mh; ++p) asum += al[p];
+        if (fabs(asum) < 1.0e-30) asum = 1.0e-30;
+        for (int p = 0; p < mh; ++p) {
+            double a = al[p] / asum;
+            if (alpha_max > 0.0) {
+                if (a < -alpha_max) a = -alpha_max;
+                if (a > alpha_max) a = alpha_max;
+            }
+            alpha_out[p] = a;
+        }
+    }
 }
 
-__device__ __forceinline__ double block_max(double v, SMem& sm, int slot) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    v = warp_max(v);
-    if (lane == 0) sm.red[warp][slot] = v;
-    __syncthreads();
-    double t = 0.0;
-    if (threadIdx.x == 0)
-        for (int w = 0; w < kWarps; ++w) t = nan_max(t, sm.red[w][slot]);
-    __syncthreads();
-    return t;
-}
-
-// ---- R(m): row reduction / W update ---------------------------------------
-__device__ void reduce_block(const ImpInst& I, int rb, int m, SMem& sm) {
-    const int k = rb * kRB + threadIdx.x;
+// ---- R(m): row reduction / W update, one warp per 32 rows -----------------
+__device__ void reduce_wunit(WarpSmem& w, int ru, int m) {
+    const ImpInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const int k = ru * kRW + lane;
     const bool ok = k < I.n_inner;
     const int i = k + 1;
-    const int d = 3 * I.n_inner;
+    const int nx = I.nx, n_inner = I.n_inner, d = 3 * n_inner;
     double wn[3] = {0.0, 0.0, 0.0}, wo[3] = {0.0, 0.0, 0.0};
     if (ok) {
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-        for (int vt = 0; vt < I.nvt; ++vt) {
-            const double* p = I.part + ((size_t)vt * I.n_inner + k) * kPartQ;
-            s0 += ld_cg(p);
-            s1 += ld_cg(p + 1);
-            s2 += ld_cg(p + 2);
-        }
+        double s0, s1, s2;
+        sum_partials(I.part, I.nvt, n_inner, k, &s0, &s1, &s2);
         moments_from_sums(s0, s1, s2, I.dv, &wn[0], &wn[1], &wn[2]);
         wo[0] = ld_cg(&I.W[i]);
-        wo[1] = ld_cg(&I.W[I.nx + i]);
-        wo[2] = ld_cg(&I.W[2 * I.nx + i]);
+        wo[1] = ld_cg(&I.W[nx + i]);
+        wo[2] = ld_cg(&I.W[2 * nx + i]);
         I.Wn[i] = wn[0];
-        I.Wn[I.nx + i] = wn[1];
-        I.Wn[2 * I.nx + i] = wn[2];
+        I.Wn[nx + i] = wn[1];
+        I.Wn[2 * nx + i] = wn[2];
     }
     // conv_type "w": bgk1d_conv_util.py:35-58 over all nx cells
     if (I.conv_type == 1) {
-        double q1 = 0.0, q2 = 0.0;
-        auto add = [&](double a, double o) {
-            const double df = fabs(a - o);
-            const double ref = nan_max(fabs(a), fabs(o));
-            q1 = nan_max(q1, df / (I.abs_tol + I.tol * ref));
-            const double rc = (ref != ref || ref >= I.abs_tol) ? ref : I.abs_tol;
-            q2 = nan_max(q2, df / rc);
-        };
-        if (ok)
-            for (int q = 0; q < 3; ++q) add(wn[q], wo[q]);
-        if (rb == 0 && threadIdx.x < 2) {
-            const int ib = threadIdx.x == 0 ? 0 : I.nx - 1;
-            for (int q = 0; q < 3; ++q) add(ld_cg(&I.Wb[3 * threadIdx.x + q]), ld_cg(&I.W[q * I.nx + ib]));
+        const double at = I.abs_tol, tl = I.tol;
+        FracMax q1, q2;
+        if (ok) {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const double df = fabs(wn[q] - wo[q]);
+                const double ref = nan_max(fabs(wn[q]), fabs(wo[q]));
+                q1.add(df, at + tl * ref);
+                q2.add(df, (ref != ref || ref >= at) ? ref : at);
+            }
         }
-        q1 = block_max(q1, sm, 0);
-        q2 = block_max(q2, sm, 1);
-        if (threadIdx.x == 0) {
-            atomic_max_nonneg(&I.res[2 * m], q1);
-            atomic_max_nonneg(&I.res[2 * m + 1], q2);
+        if (ru == 0 && lane < 2) {  // the two boundary rows
+            const int ib = lane == 0 ? 0 : nx - 1;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const double a = ld_cg(&I.Wb[3 * lane + q]), o = ld_cg(&I.W[q * nx + ib]);
+                const double df = fabs(a - o);
+                const double ref = nan_max(fabs(a), fabs(o));
+                q1.add(df, at + tl * ref);
+                q2.add(df, (ref != ref || ref >= at) ? ref : at);
+            }
+        }
+        const double r1 = warp_max(q1.value()), r2 = warp_max(q2.value());
+        if (lane == 0) {
+            atomic_max_nonneg(&I.res[2 * m], r1);
+            atomic_max_nonneg(&I.res[2 * m + 1], r2);
         }
     }
     // boundary rows: W <- floors(moments of the fixed boundary rows)
-    if (rb == 0 && threadIdx.x < 2) {
-        const int ib = threadIdx.x == 0 ? 0 : I.nx - 1;
-        I.W[ib] = clamp_min_t(ld_cg(&I.Wb[3 * threadIdx.x + 0]), 1e-12);
-        I.W[I.nx + ib] = ld_cg(&I.Wb[3 * threadIdx.x + 1]);
-        I.W[2 * I.nx + ib] = clamp_min_t(ld_cg(&I.Wb[3 * threadIdx.x + 2]), 1e-12);
+    if (ru == 0 && lane < 2) {
+        const int ib = lane == 0 ? 0 : nx - 1;
+        I.W[ib] = clamp_min_t(ld_cg(&I.Wb[3 * lane + 0]), 1e-12);
+        I.W[nx + ib] = ld_cg(&I.Wb[3 * lane + 1]);
+        I.W[2 * nx + ib] = clamp_min_t(ld_cg(&I.Wb[3 * lane + 2]), 1e-12);
     }
 
     bool plain = true;
     if (I.aa_on) {
-        // Anderson call number m (bgk1d_aa_cpu.py:7-129): history column
-        // head_in = m % cols, history length min(m+1, cols).
+        // Anderson call m: history column head_in = m % cols, length min(m+1, cols)
         const int head_in = m % I.aa_cols;
         const int mh = (m + 1) < I.aa_cols ? (m + 1) : I.aa_cols;
         const int head_out = (m + 1) % I.aa_cols;
-        const bool should = (m + 1) >= I.aa_start && ((m + 1 - I.aa_start) % I.aa_stride == 0);
-        const bool apply = should && mh >= 2;
         if (ok) {
+#pragma unroll
             for (int q = 0; q < 3; ++q) {
-                I.aaG[(size_t)head_in * d + q * I.n_inner + k] = wn[q];
-                I.aaR[(size_t)head_in * d + q * I.n_inner + k] = wn[q] - wo[q];
+                I.aaG[(size_t)head_in * d + q * n_inner + k] = wn[q];
+                I.aaR[(size_t)head_in * d + q * n_inner + k] = wn[q] - wo[q];
             }
         }
-        if (apply) {
+        if (aa_applies(I, m)) {
             plain = false;
-            __syncthreads();  // this block's history writes are its own rows only
-            int cols[kMaxAACols];
-            for (int jj = 0; jj < mh; ++jj)
-                cols[jj] = ((head_out - mh + jj) % I.aa_cols + I.aa_cols) % I.aa_cols;
-            int pi = 0;
-            for (int p = 0; p < mh; ++p)
-                for (int q = p; q < mh; ++q, ++pi) {
-                    double v = 0.0;
-                    if (ok)
-                        for (int cc = 0; cc < 3; ++cc)
-                            v += I.aaR[(size_t)cols[p] * d + cc * I.n_inner + k] *
-                                 I.aaR[(size_t)cols[q] * d + cc * I.n_inner + k];
-                    v = block_sum(v, sm, 2);
-                    if (threadIdx.x == 0) I.gpart[(size_t)rb * kMaxPairs + pi] = v;
+            double rv[kMaxAACols][3];
+#pragma unroll
+            for (int jj = 0; jj < kMaxAACols; ++jj) {
+                const int col = ((head_out - mh + jj) % I.aa_cols + I.aa_cols) % I.aa_cols;
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    rv[jj][q] = 0.0;
+                    if (ok && jj < mh)
+                        rv[jj][q] = (col == head_in) ? (wn[q] - wo[q])
+                                                     : ld_cg(&I.aaR[(size_t)col * d + q * n_inner + k]);
                 }
-            // last block of this instance assembles the Gram matrix and solves
-            if (threadIdx.x == 0) {
-                __threadfence();
-                const unsigned prev = atomicAdd(&I.rbdone[m], 1u);
-                sm.flags = (prev == (unsigned)I.nrb - 1) ? 1 : 0;
             }
-            __syncthreads();
-            if (sm.flags && threadIdx.x == 0) {
-                __threadfence();
-                double A[kMaxAACols * kMaxAACols];
-                int pj = 0;
-                for (int p = 0; p < mh; ++p)
-                    for (int q = p; q < mh; ++q, ++pj) {
-                        double s = 0.0;
-                        for (int r2 = 0; r2 < I.nrb; ++r2) s += ld_cg(&I.gpart[(size_t)r2 * kMaxPairs + pj]);
-                        A[p * mh + q] = s;
-                        A[q * mh + p] = s;
+#pragma unroll
+            for (int p = 0; p < kMaxAACols; ++p)
+#pragma unroll
+                for (int q = p; q < kMaxAACols; ++q) {
+                    if (p < mh && q < mh) {
+                        const double v = warp_sum(rv[p][0] * rv[q][0] + rv[p][1] * rv[q][1] +
+                                                  rv[p][2] * rv[q][2]);
+                        const int pi = p * mh - (p * (p - 1)) / 2 + (q - p);
+                        if (lane == 0) I.gpart[(size_t)ru * kMaxPairs + pi] = v;
                     }
-                for (int p = 0; p < mh; ++p) A[p * mh + p] += I.aa_reg;
-                double al[kMaxAACols];
-                aa_small_solve(mh, A, al);
-                double asum = 0.0;
-                for (int p = 0; p < mh; ++p) asum += al[p];
-                if (fabs(asum) < 1.0e-30) asum = 1.0e-30;
-                for (int p = 0; p < mh; ++p) {
-                    double a = al[p] / asum;
-                    if (I.aa_alpha_max > 0.0) {
-                        if (a < -I.aa_alpha_max) a = -I.aa_alpha_max;
-                        if (a > I.aa_alpha_max) a = I.aa_alpha_max;
-                    }
-                    I.alpha[(size_t)m * kMaxAACols + p] = a;
                 }
+            unsigned prev = 0;
+            if (lane == 0) {
+                fence_acq_rel();
+                prev = atomicAdd(&I.rbdone[m], 1u);
+            }
+            prev = __shfl_sync(0xffffffffu, prev, 0);
+            if (prev == (unsigned)I.nrb - 1) {
+                fence_acq_rel();
+                aa_finalize(I.gpart, I.nrb, mh, I.aa_reg, I.aa_alpha_max,
+                            I.alpha + (size_t)m * kMaxAACols);
             }
         }
     }
@@ -641,25 +705,78 @@ __device__ void reduce_block(const ImpInst& I, int rb, int m, SMem& sm) {
         const double nn = clamp_min_t(wn[0], 1e-12);
         const double TT = clamp_min_t(wn[2], 1e-12);
         I.W[i] = nn;
-        I.W[I.nx + i] = wn[1];
-        I.W[2 * I.nx + i] = TT;
+        I.W[nx + i] = wn[1];
+        I.W[2 * nx + i] = TT;
         double c4[4];
-        row_coeffs(I, nn, wn[1], TT, c4);
+        row_coeffs(I.tau_tilde, I.dt, nn, wn[1], TT, c4);
         reinterpret_cast<double2*>(&I.Wc[4 * (size_t)i])[0] = make_double2(c4[0], c4[1]);
         reinterpret_cast<double2*>(&I.Wc[4 * (size_t)i])[1] = make_double2(c4[2], c4[3]);
     }
-    if (rb == 0 && threadIdx.x == 0) I.st[m] = 1;
+    if (ru == 0 && lane == 0) I.st[m] = 1;
+}
+
+// ---- P2: W^(0) from the moment partials of f^n (one warp per 32 rows) -----
+__device__ void init_wunit(WarpSmem& w, int ru) {
+    const ImpInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const int k = ru * kRW + lane;
+    const int nx = I.nx, n_inner = I.n_inner;
+    if (k < n_inner) {
+        double s0, s1, s2;
+        sum_partials(I.part, I.nvt, n_inner, k, &s0, &s1, &s2);
+        double n, nu, T;
+        moments_from_sums(s0, s1, s2, I.dv, &n, &nu, &T);
+        const int i = k + 1;
+        I.W[i] = n;
+        I.W[nx + i] = nu;
+        I.W[2 * nx + i] = T;
+        double c4[4];
+        row_coeffs(I.tau_tilde, I.dt, n, nu, T, c4);
+        reinterpret_cast<double2*>(&I.Wc[4 * (size_t)i])[0] = make_double2(c4[0], c4[1]);
+        reinterpret_cast<double2*>(&I.Wc[4 * (size_t)i])[1] = make_double2(c4[2], c4[3]);
+    }
+    if (ru == 0 && lane < 2) {
+        const int ib = lane == 0 ? 0 : nx - 1;
+        for (int q = 0; q < 3; ++q) I.W[q * nx + ib] = ld_cg(&I.Wb[3 * lane + q]);
+    }
+}
+
+__device__ __forceinline__ void flush_residual(const ImpInst& I, int m, FracMax& q1, FracMax& q2,
+                                               bool& bad) {
+    const int lane = threadIdx.x & 31;
+    const double r1 = warp_max(q1.value()), r2 = warp_max(q2.value());
+    const bool anybad = __any_sync(0xffffffffu, bad);
+    if (lane == 0 && I.conv_type == 0) {
+        atomic_max_nonneg(&I.res[2 * m], r1);
+        atomic_max_nonneg(&I.res[2 * m + 1], r2);
+    }
+    if (lane == 0 && anybad) atomicOr(&I.nonfin[m], 1);
+    q1 = FracMax();
+    q2 = FracMax();
+    bad = false;
 }
 
 // ---- the persistent kernel --------------------------------------------------
+// Work items (warp-tiles, reduction units) are statically strided over all
+// resident warps of the cooperative grid.  Within an instance, warp-tiles are
+// numbered chunk-major (t = c*nvt + vt) and every warp visits its items in
+// increasing order, so the tile a look-back waits for has a smaller number
+// and is processed by a warp that never waits on a larger one: every wait
+// completes.
 __global__ void __launch_bounds__(kThreads, 2)
 implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
-    __shared__ SMem sm;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     PlanDev& P = *Pp;
     const unsigned G = gridDim.x;
     const int n_inst = P.n_inst;
+    const long long total_tiles = P.total_tiles, total_ru = P.total_rb;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    WarpSmem& w = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
+    const long long gwarp = (long long)blockIdx.x * kWarps + warp, nwarps = (long long)G * kWarps;
+    if (lane == 0) w.cur_b = -1;
+    __syncwarp();
 
-    // P0: reset per-step state, boundary rows of f_out
+    // P0: reset per-step state, boundary rows of f_out, boundary-row moments
     for (int b = blockIdx.x; b < n_inst; b += G) {
         const ImpInst& I = P.inst[b];
         const double* fn = swap_io ? I.f_out : I.f_in;
@@ -675,8 +792,8 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
             fo[q] = fn[q];
             fo[(size_t)(I.nx - 1) * I.nv + q] = fn[(size_t)(I.nx - 1) * I.nv + q];
         }
-        // boundary-row moments (sequential per row, C1 order)
         if (threadIdx.x < 2) {
+            // sequential per row, the C1 order
             const double* row = fn + (size_t)(threadIdx.x == 0 ? 0 : I.nx - 1) * I.nv;
             double s0 = 0.0, s1 = 0.0, s2 = 0.0;
             for (int jj = 0; jj < I.nv; ++jj) {
@@ -692,49 +809,23 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
             I.Wb[3 * threadIdx.x + 2] = T;
         }
     }
-    if (blockIdx.x == 0)
-        for (int q = threadIdx.x; q <= P.max_iter; q += kThreads) P.tickets[q] = 0u;
     if (!grid_sync(&P.bar, G, &P.err)) return;
 
     // P1: moments of f^n
-    for (long long t = blockIdx.x; t < P.total_tiles; t += G) {
+    for (long long t = gwarp; t < total_tiles; t += nwarps) {
         const int b = find_inst(P.tile_off, n_inst, t);
-        const ImpInst& I = P.inst[b];
-        const long long tl = t - I.tile_off;
-        const int c = (int)(tl / I.nvt), vt = (int)(tl % I.nvt);
-        moments_tile(I, vt, c, swap_io ? I.f_out : I.f_in);
+        stage_warp(w, &P.inst[b], b);
+        const long long tl = t - w.I.tile_off;
+        const int c = (int)(tl / w.I.nvt), vt = (int)(tl % w.I.nvt);
+        moments_wtile(w.I, vt, c, swap_io ? w.I.f_out : w.I.f_in);
     }
     if (!grid_sync(&P.bar, G, &P.err)) return;
 
     // P2: W^(0) (unfloored C1 moments) and coefficients
-    for (long long t = blockIdx.x; t < P.total_rb; t += G) {
-        const int b = find_inst(P.rb_off, n_inst, t);
-        const ImpInst& I = P.inst[b];
-        const int rb = (int)(t - I.rb_off);
-        const int k = rb * kRB + threadIdx.x;
-        if (k < I.n_inner) {
-            double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-            for (int vt = 0; vt < I.nvt; ++vt) {
-                const double* p = I.part + ((size_t)vt * I.n_inner + k) * kPartQ;
-                s0 += ld_cg(p);
-                s1 += ld_cg(p + 1);
-                s2 += ld_cg(p + 2);
-            }
-            double n, nu, T;
-            moments_from_sums(s0, s1, s2, I.dv, &n, &nu, &T);
-            const int i = k + 1;
-            I.W[i] = n;
-            I.W[I.nx + i] = nu;
-            I.W[2 * I.nx + i] = T;
-            double c4[4];
-            row_coeffs(I, n, nu, T, c4);
-            reinterpret_cast<double2*>(&I.Wc[4 * (size_t)i])[0] = make_double2(c4[0], c4[1]);
-            reinterpret_cast<double2*>(&I.Wc[4 * (size_t)i])[1] = make_double2(c4[2], c4[3]);
-        }
-        if (rb == 0 && threadIdx.x < 2) {
-            const int ib = threadIdx.x == 0 ? 0 : I.nx - 1;
-            for (int q = 0; q < 3; ++q) I.W[q * I.nx + ib] = ld_cg(&I.Wb[3 * threadIdx.x + q]);
-        }
+    for (long long u = gwarp; u < total_ru; u += nwarps) {
+        const int b = find_inst(P.rb_off, n_inst, u);
+        stage_warp(w, &P.inst[b], b);
+        init_wunit(w, (int)(u - w.I.rb_off));
     }
     if (!grid_sync(&P.bar, G, &P.err)) return;
 
@@ -743,38 +834,32 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
         bool any = false;
         for (int b = 0; b < n_inst && !any; ++b) any = inst_active(P.inst[b], m);
         if (!any) break;
-        if (__ldcg(&P.err) != 0) break;
 
         // S(m)
-        while (true) {
-            if (threadIdx.x == 0) sm.tile = (long long)atomicAdd(&P.tickets[m], 1u);
-            __syncthreads();
-            const long long t = sm.tile;
-            __syncthreads();
-            if (t >= P.total_tiles) break;
+        FracMax q1, q2;
+        bool bad = false;
+        int res_b = -1;
+        for (long long t = gwarp; t < total_tiles; t += nwarps) {
             const int b = find_inst(P.tile_off, n_inst, t);
-            const ImpInst& I = P.inst[b];
-            if (!inst_active(I, m)) continue;
-            const long long tl = t - I.tile_off;
-            const int c = (int)(tl / I.nvt), vt = (int)(tl % I.nvt);
-            // Anderson weights of the previous call, if it applied
-            if (I.aa_on && m >= 1 && threadIdx.x < kMaxAACols)
-                sm.alpha[threadIdx.x] = ld_cg(&I.alpha[(size_t)(m - 1) * kMaxAACols + threadIdx.x]);
-            __syncthreads();
-            const double* fn = swap_io ? I.f_out : I.f_in;
-            double* fo = swap_io ? const_cast<double*>(I.f_in) : I.f_out;
-            solve_tile(&P.err, I, vt, c, m, sm, fn, fo);
-            __syncthreads();
+            if (b != res_b && res_b >= 0) flush_residual(w.I, m, q1, q2, bad);
+            stage_warp(w, &P.inst[b], b);
+            res_b = b;
+            if (!inst_active(w.I, m)) continue;
+            const long long tl = t - w.I.tile_off;
+            const int c = (int)(tl / w.I.nvt), vt = (int)(tl % w.I.nvt);
+            const double* fn = swap_io ? w.I.f_out : w.I.f_in;
+            double* fo = swap_io ? const_cast<double*>(w.I.f_in) : w.I.f_out;
+            solve_wtile(&P.err, w, vt, c, m, fn, fo, q1, q2, bad);
         }
+        if (res_b >= 0 && inst_active(w.I, m)) flush_residual(w.I, m, q1, q2, bad);
         if (!grid_sync(&P.bar, G, &P.err)) return;
 
         // R(m)
-        for (long long t = blockIdx.x; t < P.total_rb; t += G) {
-            const int b = find_inst(P.rb_off, n_inst, t);
-            const ImpInst& I = P.inst[b];
-            if (!inst_active(I, m)) continue;
-            reduce_block(I, (int)(t - I.rb_off), m, sm);
-            __syncthreads();
+        for (long long u = gwarp; u < total_ru; u += nwarps) {
+            const int b = find_inst(P.rb_off, n_inst, u);
+            stage_warp(w, &P.inst[b], b);
+            if (!inst_active(w.I, m)) continue;
+            reduce_wunit(w, (int)(u - w.I.rb_off), m);
         }
         if (!grid_sync(&P.bar, G, &P.err)) return;
     }
@@ -790,15 +875,11 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
         }
         keq_step_stats* s = I.stats;
         int aa_applied = 0;
-        if (I.aa_on)
-            for (int m = 0; m < last; ++m) {
-                const int mh = (m + 1) < I.aa_cols ? (m + 1) : I.aa_cols;
-                const bool should = (m + 1) >= I.aa_start && ((m + 1 - I.aa_start) % I.aa_stride == 0);
-                if (should && mh >= 2) ++aa_applied;
-            }
+        for (int m = 0; m < last; ++m)
+            if (aa_applies(I, m)) ++aa_applied;
         int status = KEQ_OK;
         if (last >= 0 && __ldcg(&I.nonfin[last])) status = KEQ_ERR_NONFINITE;
-        if (P.err & (1 << KEQ_ERR_TIMEOUT)) status = KEQ_ERR_TIMEOUT;
+        if (__ldcg(&P.err) & (1 << KEQ_ERR_TIMEOUT)) status = KEQ_ERR_TIMEOUT;
         s->status = status;
         s->iters = last + 1;
         s->aa_applied = aa_applied;
@@ -812,6 +893,8 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
         s->total_steps += 1;
     }
 }
+
+constexpr size_t kSmemBytes = sizeof(WarpSmem) * kWarps;
 
 }  // namespace keq
 
@@ -847,8 +930,8 @@ Derived derive(int nx, int nv, int kp, const keq_implicit_params& p) {
     d.nt_neg = (kp + 31) / 32;
     d.nt_pos = (nv - kp + 31) / 32;
     d.nvt = d.nt_neg + d.nt_pos;
-    d.nchunks = (d.n_inner + keq::kLX - 1) / keq::kLX;
-    d.nrb = (d.n_inner + keq::kRB - 1) / keq::kRB;
+    d.nchunks = (d.n_inner + keq::kR - 1) / keq::kR;
+    d.nrb = (d.n_inner + keq::kRW - 1) / keq::kRW;
     const int aa_m = p.aa_m > 0 ? p.aa_m : 0;
     d.aa_on = (p.aa_enable && aa_m >= 1 && aa_m + 1 >= 2) ? 1 : 0;
     d.aa_cols = d.aa_on ? aa_m + 1 : 1;
@@ -1101,15 +1184,16 @@ keq_status keq_implicit_plan_create(const keq_instance* insts, int32_t n,
     int dev_id = 0, sms = 0, occ = 0;
     cudaGetDevice(&dev_id);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, keq::implicit_step_kernel, kThreads, 0);
+    cudaFuncSetAttribute(keq::implicit_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)keq::kSmemBytes);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, keq::implicit_step_kernel, kThreads,
+                                                  keq::kSmemBytes);
     if (occ < 1 || sms < 1) {
         delete plan;
         return KEQ_ERR_UNSUPPORTED;
     }
-    long long work = toff > roff ? toff : roff;
-    long long g = (long long)sms * occ;
-    if (work < g) g = work > 0 ? work : 1;
-    plan->grid = (int)g;
+    // every resident CTA takes part: work items are strided over all warps
+    plan->grid = sms * occ;
     *plan_out = plan;
     return KEQ_OK;
 }
@@ -1145,7 +1229,7 @@ keq_status keq_plan_step(keq_plan* plan, int32_t n_steps, int32_t parity, keq_st
         void* args[] = {&plan->dev, &swap_io};
         cudaError_t e = cudaLaunchCooperativeKernel((const void*)keq::implicit_step_kernel,
                                                     dim3(plan->grid), dim3(keq::kThreads), args,
-                                                    0, s);
+                                                    keq::kSmemBytes, s);
         if (e != cudaSuccess) {
             keq_internal_set_cuda_error(e);
             return KEQ_ERR_CUDA;
