@@ -154,6 +154,13 @@ keq_status keq_plan_set_buffers(keq_plan* plan, const double* const* f_in,
  * even, and the reverse when it is odd, so the state ping-pongs between the
  * two buffers without copies; the caller tracks where the newest state is. */
 keq_status keq_plan_step(keq_plan* plan, int32_t n_steps, int32_t parity, keq_stream_t stream);
+/* Attach (iters > 0) or detach (iters = 0) a phase trace: a device buffer of
+ * iters * 4 uint64 that the caller initialises with {UINT64_MAX, 0,
+ * UINT64_MAX, 0} per row; each step then records, per Picard iteration, the
+ * earliest start and latest end (%globaltimer ns) of pass 1 and pass 2 over
+ * all warps.  No reference counterpart (profiling aid). */
+keq_status keq_plan_set_trace(keq_plan* plan, unsigned long long* trace, int32_t iters,
+                              keq_stream_t stream);
 /* Device-side error bits of the plan (1 << keq_status), synchronising the
  * stream; 0 when every device-side wait completed. */
 keq_status keq_plan_error(keq_plan* plan, keq_stream_t stream, int32_t* err_bits);
@@ -203,6 +210,13 @@ keq_status keq_block_tridiag_solve(const double* A, const double* B, const doubl
                                    const double* D, double* X, int32_t n, int32_t batch,
                                    void* workspace, size_t workspace_bytes,
                                    keq_stream_t stream);
+
+/* Numerical self-test of the device math used by the fused kernels (no
+ * reference counterpart): kind 0 evaluates the branch-free e^x for x <= 0,
+ * kind 1 the Newton reciprocal 1/x for x >= 1, element-wise on device
+ * arrays x -> y. */
+keq_status keq_math_selftest(int32_t kind, const double* x, double* y, int32_t n,
+                             keq_stream_t stream);
 
 #ifdef __cplusplus
 }

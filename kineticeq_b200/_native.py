@@ -86,6 +86,7 @@ _PROTOS = {
     "keq_plan_set_buffers": (_i32, [_vp, C.POINTER(_vp), C.POINTER(_vp), _vp]),
     "keq_plan_step": (_i32, [_vp, _i32, _i32, _vp]),
     "keq_plan_error": (_i32, [_vp, _vp, C.POINTER(_i32)]),
+    "keq_plan_set_trace": (_i32, [_vp, _vp, _i32, _vp]),
     "keq_plan_destroy": (None, [_vp]),
     "keq_implicit_workspace_size": (_i32, [C.POINTER(Grid), C.POINTER(ImplicitParams),
                                            C.POINTER(_sz)]),
@@ -98,6 +99,7 @@ _PROTOS = {
     "keq_gtsv_strided_inplace": (_i32, [_dp, _dp, _dp, _dp, _i32, _i32, _vp, _sz, _vp]),
     "keq_block_tridiag_workspace_size": (_i32, [_i32, _i32, C.POINTER(_sz)]),
     "keq_block_tridiag_solve": (_i32, [_dp, _dp, _dp, _dp, _dp, _i32, _i32, _vp, _sz, _vp]),
+    "keq_math_selftest": (_i32, [_i32, _dp, _dp, _i32, _vp]),
 }
 
 # Entry points that are declared in the header but may be added by later

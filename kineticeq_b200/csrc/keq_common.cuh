@@ -56,6 +56,60 @@ __device__ __forceinline__ double recip_nr(double d) {
     return fma(r, e, r);
 }
 
+// 1/d for d >= 1 (the implicit diagonal 1 + alpha + beta + dt/tau), branch
+// and conversion free: Newton-Raphson r <- r + r (1 - d r) twice from the
+// hardware reciprocal approximation rcp.approx.ftz.f64 (relative error below
+// 2^-20, so two steps leave < 2^-80 before the final rounding).
+__device__ __forceinline__ double recip_ge1(double d) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+    double e = fma(-d, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-d, r, 1.0);
+    return fma(r, e, r);
+}
+
+// e^x for x <= 0, branch and conversion free (so that independent
+// evaluations interleave at full FP64 issue rate).  Cody-Waite argument
+// reduction x = k ln2 + r with ln2 split into a 32-bit head (exact products
+// k*LN2_HI for |k| < 2^21) and a tail, |r| <= ln2/2; k is rounded with the
+// 1.5*2^52 addition trick and read from the low word of the sum; then the
+// degree-13 Taylor polynomial of e^r (truncation < 5e-18 relative) by Horner's
+// rule, and the scale 2^k built in the exponent field (two factors below
+// 2^-1000 so that subnormal results round once).  NaN propagates, -inf and
+// x < -745.5 give 0.  Accuracy is checked against CUDA's exp in the tests.
+__device__ __forceinline__ double exp_nonpos(double x) {
+    constexpr double LOG2E = 1.4426950408889634;
+    constexpr double LN2_HI = 0.6931471806019545;       // 0x3fe62e42ff000000
+    constexpr double LN2_LO = -4.2009150726810846e-11;  // ln2 - LN2_HI
+    constexpr double ROUND = 6755399441055744.0;         // 1.5 * 2^52
+    const double xc = (x < -745.5) ? -745.5 : x;
+    const double kr = fma(xc, LOG2E, ROUND);              // k in the low mantissa bits
+    const int ki = __double2loint(kr);                    // k in [-1076, 0]
+    const double k = kr - ROUND;
+    double r = fma(-k, LN2_HI, xc);
+    r = fma(-k, LN2_LO, r);
+    double p = 1.6059043836821613e-10;   // 1/13!
+    p = fma(p, r, 2.08767569878681e-09);  // 1/12!
+    p = fma(p, r, 2.505210838544172e-08);
+    p = fma(p, r, 2.755731922398589e-07);
+    p = fma(p, r, 2.7557319223985893e-06);
+    p = fma(p, r, 2.48015873015873e-05);
+    p = fma(p, r, 0.0001984126984126984);
+    p = fma(p, r, 0.001388888888888889);
+    p = fma(p, r, 0.008333333333333333);
+    p = fma(p, r, 0.041666666666666664);
+    p = fma(p, r, 0.16666666666666666);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.0);
+    p = fma(p, r, 1.0);
+    const bool sub = ki < -1000;
+    const int e1 = sub ? ki + 60 : ki;
+    const double s1 = __hiloint2double((e1 + 1023) << 20, 0);
+    const double s2 = sub ? 8.673617379884035e-19 : 1.0;  // 2^-60
+    return (p * s1) * s2;
+}
+
 // Running maximum of ratios num/den without a division per element: the
 // maximum is kept as a fraction and compared by cross-multiplication
 // (num_a * den_b > num_b * den_a for positive finite denominators).

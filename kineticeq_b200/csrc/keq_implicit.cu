@@ -47,10 +47,9 @@
 
 namespace keq {
 
-constexpr int kWarps = 8;                // warps per CTA
+constexpr int kWarps = 4;                // warps per CTA
 constexpr int kThreads = kWarps * 32;
-constexpr int kR = 16;                   // scan positions (rows) per warp-tile
-constexpr int kRW = 32;                  // rows per reduction warp unit
+constexpr int kR = 32;                   // rows (scan positions) per warp-tile = rows per row block
 constexpr int kMaxAACols = 8;            // Anderson ring columns (aa_m <= 7)
 constexpr int kMaxPairs = kMaxAACols * (kMaxAACols + 1) / 2;
 constexpr int kPartQ = 4;                // doubles per (v-tile,row) partial
@@ -74,8 +73,11 @@ struct ImpInst {
     double* Wc;      // 4*nx  : per-row (u, -1/(2T), n/sqrt(2 pi T), dt/tau)
     double* Wb;      // 8     : moments of the two boundary rows
     double* part;    // nvt*n_inner*kPartQ
-    double* lb;      // nvt*nchunks*3*32  (P | Y | X per lane)
-    unsigned* lbflag;// nvt*nchunks
+    double* agg;     // nvt*nchunks*64 : tile maps (P | Y per lane)
+    double* gmap;    // nvt*ngroups*64 : composed maps of groups of chunks
+    double* crhs;    // nx*nv : scaled right-hand side c = b/d of the current iterate
+    unsigned* grpcnt;// picard_iter*nvt*ngroups : tiles of a chunk group done (pass 1)
+    unsigned* rbcnt; // picard_iter*nrb  : rows x v-tiles of a row block done (pass 2)
     double* res;     // 2*picard_iter : std / rel residual slots
     int* st;         // picard_iter   : 1 if active in iteration m
     int* nonfin;     // picard_iter   : non-finite flag of iterate m+1
@@ -98,17 +100,18 @@ struct PlanDev {
     long long* tile_off;  // n_inst+1
     long long* rb_off;    // n_inst+1
     unsigned* tickets;    // max_iter+1 (reserved)
+    unsigned long long* trace;  // optional: kTracePhases stamps per iteration (ns)
+    int trace_iters;
 };
 
-// Per-warp shared memory: the instance descriptor of the warp's current work
-// item, the f^n tile / local solution, the local propagator and the row
-// coefficients.
+// Per-warp shared memory.
 struct WarpSmem {
     ImpInst I;
-    double fy[kR][32];     // f^n of the warp-tile, then the local solution y
-    double fP[kR][32];     // local propagator P (x = y + P * carry)
+    double buf0[kR][32];   // pass 1: f^n tile; pass 2: c tile
+    double buf1[kR][32];   // pass 2: previous iterate (residual reference)
     double coef[kR][4];    // (u, -1/(2T), n/sqrt(2 pi T), dt/tau) per row
     int cur_b;
+    int done_rb[2];
     int pad;
 };
 
@@ -250,13 +253,13 @@ __device__ __forceinline__ void stage_warp(WarpSmem& w, const ImpInst* src, int 
     __syncwarp();
 }
 
-// Warp reduce-scatter of the 3 moments of kR rows held per lane, in two
-// halves of kR/2 rows, and store of the per-(v-tile,row) partials.
-__device__ __forceinline__ void store_partials(const ImpInst& I, const TileGeo& g, int vt, int lane,
-                                               double (&acc)[kR / 2 * 3], int half) {
-    warp_reduce_scatter<kR / 2, 3>(acc, lane);
-    if (owner_writes<kR / 2>(lane)) {
-        const int s = g.s0 + half * (kR / 2) + owner_row<kR / 2>(lane);
+// Reduce-scatter of the 3 moments of 8 rows held per lane and store of the
+// per-(v-tile,row) partials; rows s0 + 8*q8 .. +7.
+__device__ __forceinline__ void store_partials8(const ImpInst& I, const TileGeo& g, int vt, int lane,
+                                                double (&acc)[24], int q8) {
+    warp_reduce_scatter<8, 3>(acc, lane);
+    if (owner_writes<8>(lane)) {
+        const int s = g.s0 + 8 * q8 + owner_row<8>(lane);
         if (s < I.n_inner) {
             const int k = scan_row(I.nx, g.pos, s) - 1;
             double* p = I.part + ((size_t)vt * I.n_inner + k) * kPartQ;
@@ -272,206 +275,318 @@ __device__ void moments_wtile(const ImpInst& I, int vt, int c, const double* __r
     const int lane = threadIdx.x & 31;
     const TileGeo g = tile_geo(I, vt, c, lane);
     const double vj = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
+#pragma unroll 1
+    for (int q8 = 0; q8 < kR / 8; ++q8) {
+        double acc[24];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        double acc[kR / 2 * 3];
-#pragma unroll
-        for (int r = 0; r < kR / 2; ++r) {
-            const int s = g.s0 + h * (kR / 2) + r;
+        for (int r = 0; r < 8; ++r) {
+            const int s = g.s0 + 8 * q8 + r;
             double x = 0.0;
             if (s < I.n_inner && g.lane_ok) x = f[(size_t)scan_row(I.nx, g.pos, s) * I.nv + g.j];
             acc[3 * r + 0] = x;
             acc[3 * r + 1] = x * vj;
             acc[3 * r + 2] = x * vj * vj;
         }
-        store_partials(I, g, vt, lane, acc, h);
+        store_partials8(I, g, vt, lane, acc, q8);
     }
 }
 
-// ---- S(m): fused solve of one warp-tile (32 velocities x kR rows) --------
-__device__ void solve_wtile(int* err, WarpSmem& w, int vt, int c, int m,
-                            const double* __restrict__ fn, double* __restrict__ fo, FracMax& q1,
-                            FracMax& q2, bool& bad) {
+// Row coefficients of W^(m) for the warp-tile's rows into w.coef (lane r
+// handles row r).  After an applied Anderson call the combination
+// w = beta G alpha + (1-beta) w_new with floors and |u| <= u_max
+// (bgk1d_aa_cpu.py:170-188) is formed from the history ring; tiles of v-tile 0
+// then publish W^(m) and its coefficients for pass 2 and the reduction.
+__device__ __forceinline__ void stage_coeffs(WarpSmem& w, const TileGeo& g, int vt, int m,
+                                             bool pass1) {
+    const ImpInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const int nx = I.nx, n_inner = I.n_inner;
+    const int s = g.s0 + lane;
+    double c4[4] = {0.0, 0.0, 0.0, 0.0};
+    if (s < n_inner) {
+        const int i = scan_row(nx, g.pos, s);
+        if (pass1 && m >= 1 && aa_applies(I, m - 1)) {
+            const int k = i - 1, d = 3 * n_inner;
+            const int mh = m < I.aa_cols ? m : I.aa_cols;
+            const int head_out = m % I.aa_cols;
+            double al[kMaxAACols];
+            int col[kMaxAACols];
+#pragma unroll
+            for (int jj = 0; jj < kMaxAACols; ++jj) {
+                al[jj] = jj < mh ? ld_cg(&I.alpha[(size_t)(m - 1) * kMaxAACols + jj]) : 0.0;
+                col[jj] = ((head_out - mh + jj) % I.aa_cols + I.aa_cols) % I.aa_cols;
+            }
+            double wv[3];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                double gv[kMaxAACols];
+#pragma unroll
+                for (int jj = 0; jj < kMaxAACols; ++jj)
+                    gv[jj] = jj < mh ? ld_cg(&I.aaG[(size_t)col[jj] * d + q * n_inner + k]) : 0.0;
+                double acc = 0.0;
+#pragma unroll
+                for (int jj = 0; jj < kMaxAACols; ++jj)
+                    if (jj < mh) acc += gv[jj] * al[jj];
+                const double wnew = ld_cg(&I.Wn[q * nx + i]);
+                wv[q] = acc * I.aa_beta + (1.0 - I.aa_beta) * wnew;
+            }
+            const double nm = clamp_min_t(wv[0], 1e-12);
+            const double Tm = clamp_min_t(wv[2], 1e-12);
+            double um = wv[1] / nm;
+            if (!isfinite(um)) um = 0.0;
+            um = um < -I.u_max ? -I.u_max : (um > I.u_max ? I.u_max : um);
+            const double num = nm * um;
+            row_coeffs(I.tau_tilde, I.dt, nm, num, Tm, c4);
+            if (vt == 0) {
+                I.W[i] = nm;
+                I.W[nx + i] = num;
+                I.W[2 * nx + i] = Tm;
+                reinterpret_cast<double2*>(&I.Wc[4 * (size_t)i])[0] = make_double2(c4[0], c4[1]);
+                reinterpret_cast<double2*>(&I.Wc[4 * (size_t)i])[1] = make_double2(c4[2], c4[3]);
+            }
+        } else {
+            const double2 c01 = __ldcg(reinterpret_cast<const double2*>(&I.Wc[4 * (size_t)i]));
+            const double2 c23 = __ldcg(reinterpret_cast<const double2*>(&I.Wc[4 * (size_t)i + 2]));
+            c4[0] = c01.x; c4[1] = c01.y; c4[2] = c23.x; c4[3] = c23.y;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) w.coef[lane][q] = c4[q];
+}
+
+// ---- pass 1: the affine map x_out = P x_in + Y of one warp-tile ------------
+// For v > 0 the upwind implicit row is x_i = (b_i + alpha x_{i-1}) / d_i with
+// d_i = 1 + alpha + dt/tau_i and b_i = f^n_i + dt/tau_i M_i(v)
+// (implicit_kernels.cu:104-131); v <= 0 is the mirror image in x.  Written as
+// x_s = a_s x_{s-1} + c_s with a_s = alpha/d_s, c_s = b_s/d_s.  Pass 1 stores
+// c (the only part that needs the Maxwellian) and the tile map; the last tile
+// of each group of kGroup chunks of a velocity column also stores the
+// group's composed map.
+constexpr int kGroup = 8;
+
+__device__ __forceinline__ void load_rows8(double (&v)[8], const double* __restrict__ src,
+                                           const TileGeo& g, int q8, int nx, int nv,
+                                           int n_inner) {
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const int s = g.s0 + 8 * q8 + t;
+        v[t] = (s < n_inner && g.lane_ok) ? src[(size_t)scan_row(nx, g.pos, s) * nv + g.j] : 0.0;
+    }
+}
+
+// Asynchronous copy of a warp-tile (kR rows x 32 velocities) into shared
+// memory, one 8-byte element per lane and row (all rows in flight at once).
+__device__ __forceinline__ void stage_tile(double (&dst)[kR][32], const double* __restrict__ src,
+                                           const TileGeo& g, int nx, int nv, int n_inner) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll 8
+    for (int r = 0; r < kR; ++r) {
+        const int s = g.s0 + r;
+        if (s < n_inner && g.lane_ok)
+            cp_async8(&dst[r][lane], src + (size_t)scan_row(nx, g.pos, s) * nv + g.j);
+    }
+}
+
+__device__ void map_wtile(WarpSmem& w, int vt, int c, int m, const double* __restrict__ fn) {
     const ImpInst& I = w.I;
     const int lane = threadIdx.x & 31;
     const TileGeo g = tile_geo(I, vt, c, lane);
     const int nx = I.nx, nv = I.nv, n_inner = I.n_inner, nvt = I.nvt;
-    const size_t tile_id = (size_t)c * nvt + vt;
-    const unsigned f_agg = 2u * (unsigned)m + 1u, f_inc = 2u * (unsigned)m + 2u;
-
-    // 1. f^n tile -> shared memory (asynchronous copy); the previous iterate
-    //    -> registers (this warp wrote it in the previous iteration: tiles are
-    //    statically assigned); the boundary carry.
-    double fold[kR];
-#pragma unroll
-    for (int r = 0; r < kR; ++r) {
-        const int s = g.s0 + r;
-        fold[r] = 0.0;
-        if (s < n_inner && g.lane_ok) {
-            const size_t idx = (size_t)scan_row(nx, g.pos, s) * nv + g.j;
-            cp_async8(&w.fy[r][lane], fn + idx);
-            if (m > 0) fold[r] = fo[idx];
-        }
-    }
+    stage_tile(w.buf0, fn, g, nx, nv, n_inner);
     cp_async_commit();
     const double vj = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
-    const double Xb = (c == 0 && g.lane_ok) ? fn[(size_t)(g.pos ? 0 : nx - 1) * nv + g.j] : 0.0;
-
-    // 2. row coefficients of W^(m) (lane r handles row r).  After an applied
-    //    Anderson call the combination w = beta G alpha + (1-beta) w_new,
-    //    floors and |u| <= u_max (bgk1d_aa_cpu.py:170-188) is formed here
-    //    from the history ring.
-    if (lane < kR) {
-        const int s = g.s0 + lane;
-        double c4[4] = {0.0, 0.0, 0.0, 0.0};
-        if (s < n_inner) {
-            const int i = scan_row(nx, g.pos, s);
-            if (m >= 1 && aa_applies(I, m - 1)) {
-                const int k = i - 1, d = 3 * n_inner;
-                const int mh = m < I.aa_cols ? m : I.aa_cols;
-                const int head_out = m % I.aa_cols;
-                double al[kMaxAACols];
-                int col[kMaxAACols];
-#pragma unroll
-                for (int jj = 0; jj < kMaxAACols; ++jj) {
-                    al[jj] = jj < mh ? ld_cg(&I.alpha[(size_t)(m - 1) * kMaxAACols + jj]) : 0.0;
-                    col[jj] = ((head_out - mh + jj) % I.aa_cols + I.aa_cols) % I.aa_cols;
-                }
-                double wv[3];
-#pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    double gv[kMaxAACols];
-#pragma unroll
-                    for (int jj = 0; jj < kMaxAACols; ++jj)
-                        gv[jj] = jj < mh ? ld_cg(&I.aaG[(size_t)col[jj] * d + q * n_inner + k]) : 0.0;
-                    double acc = 0.0;
-#pragma unroll
-                    for (int jj = 0; jj < kMaxAACols; ++jj)
-                        if (jj < mh) acc += gv[jj] * al[jj];
-                    const double wnew = ld_cg(&I.Wn[q * nx + i]);
-                    wv[q] = acc * I.aa_beta + (1.0 - I.aa_beta) * wnew;
-                }
-                const double nm = clamp_min_t(wv[0], 1e-12);
-                const double Tm = clamp_min_t(wv[2], 1e-12);
-                double um = wv[1] / nm;
-                if (!isfinite(um)) um = 0.0;
-                um = um < -I.u_max ? -I.u_max : (um > I.u_max ? I.u_max : um);
-                const double num = nm * um;
-                row_coeffs(I.tau_tilde, I.dt, nm, num, Tm, c4);
-                if (vt == 0) {
-                    I.W[i] = nm;
-                    I.W[nx + i] = num;
-                    I.W[2 * nx + i] = Tm;
-                }
-            } else {
-                const double2 c01 = __ldcg(reinterpret_cast<const double2*>(&I.Wc[4 * (size_t)i]));
-                const double2 c23 = __ldcg(reinterpret_cast<const double2*>(&I.Wc[4 * (size_t)i + 2]));
-                c4[0] = c01.x; c4[1] = c01.y; c4[2] = c23.x; c4[3] = c23.y;
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) w.coef[lane][q] = c4[q];
-    }
+    stage_coeffs(w, g, vt, m, true);
     cp_async_wait_all();
     __syncwarp();
-
-    // 3. Maxwellian + assembly + local solve; y and P to shared memory
     const double cpl = I.dtdx * fabs(vj);  // alpha (v>0) or beta (v<0)
     const double one_plus = 1.0 + cpl;     // 1 + alpha + beta
-    double Pseg = 1.0, Yseg = 0.0;
+    double P = 1.0, Y = 0.0;
+#pragma unroll 1
+    for (int q8 = 0; q8 < kR / 8; ++q8) {
+        double av[8], cv[8];
 #pragma unroll
-    for (int r = 0; r < kR; ++r) {
-        const int s = g.s0 + r;
-        if (s < n_inner && g.lane_ok) {
-            const double fin = w.fy[r][lane];
-            if (m == 0) fold[r] = fin;
-            const double u = w.coef[r][0], nh = w.coef[r][1];
-            const double cm = w.coef[r][2], dti = w.coef[r][3];
-            const double diff = vj - u;
-            const double M = cm * exp(diff * diff * nh);
-            const double b = fma(dti, M, fin);
-            const double rr = recip_nr(one_plus + dti);
-            Yseg = fma(cpl, Yseg, b) * rr;
-            Pseg = Pseg * (cpl * rr);
+        for (int t = 0; t < 8; ++t) {
+            const int r = 8 * q8 + t;
+            const double diff = vj - w.coef[r][0];
+            const double dti = w.coef[r][3];
+            const double M = w.coef[r][2] * exp_nonpos(diff * diff * w.coef[r][1]);
+            const double rr = recip_ge1(one_plus + dti);
+            cv[t] = fma(dti, M, w.buf0[r][lane]) * rr;
+            av[t] = cpl * rr;
         }
-        w.fy[r][lane] = Yseg;
-        w.fP[r][lane] = Pseg;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const int s = g.s0 + 8 * q8 + t;
+            if (s < n_inner && g.lane_ok) {
+                I.crhs[(size_t)scan_row(nx, g.pos, s) * nv + g.j] = cv[t];
+                Y = fma(av[t], Y, cv[t]);
+                P = P * av[t];
+            }
+        }
     }
+    const size_t tid = (size_t)c * nvt + vt;
+    I.agg[tid * 64 + lane] = P;
+    I.agg[tid * 64 + 32 + lane] = Y;
 
-    // 4. publish the tile map, decoupled look-back, publish the inclusive carry
-    double* lbt = I.lb + tile_id * 96;
-    double X = Xb;
-    if (c == 0) {
-        lbt[64 + lane] = fma(Pseg, X, Yseg);
+    // last tile of this group of chunks composes the group map (nested, in x order)
+    const int grp = c / kGroup, ngroups = (I.nchunks + kGroup - 1) / kGroup;
+    fence_acq_rel();
+    __syncwarp();
+    unsigned prev = 0;
+    if (lane == 0) prev = atomicAdd(&I.grpcnt[((size_t)m * nvt + vt) * ngroups + grp], 1u);
+    prev = __shfl_sync(0xffffffffu, prev, 0);
+    const int c0 = grp * kGroup, c1 = (c0 + kGroup < I.nchunks ? c0 + kGroup : I.nchunks);
+    if (prev == (unsigned)(c1 - c0) - 1) {
         fence_acq_rel();
         __syncwarp();
-        if (lane == 0) st_release(&I.lbflag[tile_id], f_inc);
-    } else {
-        lbt[lane] = Pseg;
-        lbt[32 + lane] = Yseg;
-        fence_acq_rel();
-        __syncwarp();
-        if (lane == 0) st_release(&I.lbflag[tile_id], f_agg);
-        int k0 = -1;  // nearest predecessor chunk with an inclusive value
-        bool ok = true;
-        for (int base = c - 1; base >= 0; base -= 32) {
-            const int kk = base - lane;
-            unsigned fl = f_inc;  // chunks < 0: the boundary acts as inclusive
-            if (kk >= 0) {
-                const unsigned* fp = &I.lbflag[(size_t)kk * nvt + vt];
-                if (!wait_flag_geq(fp, f_agg, err)) ok = false;
-                fl = ld_acquire(fp);
-            }
-            if (!__all_sync(0xffffffffu, ok)) { ok = false; break; }
-            const unsigned incl = __ballot_sync(0xffffffffu, fl >= f_inc);
-            if (incl) {
-                k0 = base - (__ffs(incl) - 1);
-                break;
+        double Pk[kGroup], Yk[kGroup];
+#pragma unroll
+        for (int q = 0; q < kGroup; ++q) {
+            Pk[q] = 1.0;
+            Yk[q] = 0.0;
+            if (c0 + q < c1) {
+                const double* a = I.agg + ((size_t)(c0 + q) * nvt + vt) * 64;
+                Pk[q] = ld_cg(a + lane);
+                Yk[q] = ld_cg(a + 32 + lane);
             }
         }
-        if (!ok) {
-            X = 0.0;
-        } else {
-            X = k0 >= 0 ? ld_cg(&I.lb[((size_t)k0 * nvt + vt) * 96 + 64 + lane])
-                        : (g.lane_ok ? fn[(size_t)(g.pos ? 0 : nx - 1) * nv + g.j] : 0.0);
-            for (int k = k0 + 1; k < c; ++k) {
-                const double* q = I.lb + ((size_t)k * nvt + vt) * 96;
-                X = fma(ld_cg(q + lane), X, ld_cg(q + 32 + lane));
+        double GP = 1.0, GY = 0.0;
+#pragma unroll
+        for (int q = 0; q < kGroup; ++q) {
+            if (c0 + q < c1) {
+                GY = fma(Pk[q], GY, Yk[q]);
+                GP = Pk[q] * GP;
             }
         }
-        lbt[64 + lane] = fma(Pseg, X, Yseg);
-        fence_acq_rel();
-        __syncwarp();
-        if (lane == 0) st_release(&I.lbflag[tile_id], f_inc);
+        double* gm = I.gmap + ((size_t)vt * ngroups + grp) * 64;
+        gm[lane] = GP;
+        gm[32 + lane] = GY;
     }
+    __syncwarp();
+}
 
-    // 5. final values, residual (bgk1d_conv_util.py:25-33), non-finite
-    //    check, partial moments
+// Carry into chunk c of column vt: the boundary value pushed through the
+// group maps of the groups before c's group, then through the chunk maps of
+// c's group before c -- a fixed nested order, so every tile (and every run)
+// gets the same value.
+__device__ __forceinline__ double tile_carry(const ImpInst& I, const TileGeo& g, int vt, int c,
+                                             const double* __restrict__ fn) {
+    const int lane = threadIdx.x & 31;
+    const int nvt = I.nvt, ngroups = (I.nchunks + kGroup - 1) / kGroup;
+    const int grp = c / kGroup;
+    double X = g.lane_ok ? fn[(size_t)(g.pos ? 0 : I.nx - 1) * I.nv + g.j] : 0.0;
+    for (int g0 = 0; g0 < grp; g0 += 8) {
+        double Pq[8], Yq[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            Pq[q] = 1.0;
+            Yq[q] = 0.0;
+            if (g0 + q < grp) {
+                const double* gm = I.gmap + ((size_t)vt * ngroups + g0 + q) * 64;
+                Pq[q] = ld_cg(gm + lane);
+                Yq[q] = ld_cg(gm + 32 + lane);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            if (g0 + q < grp) X = fma(Pq[q], X, Yq[q]);
+    }
+    const int c0 = grp * kGroup;
+    double Pk[kGroup], Yk[kGroup];
+#pragma unroll
+    for (int q = 0; q < kGroup; ++q) {
+        Pk[q] = 1.0;
+        Yk[q] = 0.0;
+        if (c0 + q < c) {
+            const double* a = I.agg + ((size_t)(c0 + q) * nvt + vt) * 64;
+            Pk[q] = ld_cg(a + lane);
+            Yk[q] = ld_cg(a + 32 + lane);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < kGroup; ++q)
+        if (c0 + q < c) X = fma(Pk[q], X, Yk[q]);
+    return X;
+}
+
+// ---- pass 2: solve of one warp-tile from its carry; residual, moments -----
+// Re-forms a_s (no exponential) and reads c_s; returns (in w.done_rb) the
+// row blocks this tile completed.
+__device__ void solve_wtile(WarpSmem& w, int vt, int c, int m, const double* __restrict__ fn,
+                            double* __restrict__ fo, FracMax& q1, FracMax& q2, bool& bad) {
+    const ImpInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const TileGeo g = tile_geo(I, vt, c, lane);
+    const int nx = I.nx, nv = I.nv, n_inner = I.n_inner;
+    // residual reference: f^(m) (this kernel's previous iterate), or f^n at m = 0
+    const double* fref = m > 0 ? fo : fn;
+    stage_tile(w.buf0, I.crhs, g, nx, nv, n_inner);
+    stage_tile(w.buf1, fref, g, nx, nv, n_inner);
+    cp_async_commit();
+    const double vj = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
+    stage_coeffs(w, g, vt, m, false);
+    double X = tile_carry(I, g, vt, c, fn);
+    cp_async_wait_all();
+    __syncwarp();
+    const double cpl = I.dtdx * fabs(vj);
+    const double one_plus = 1.0 + cpl;
     const double tol = I.tol, abs_tol = I.abs_tol;
+#pragma unroll 1
+    for (int q4 = 0; q4 < kR / 4; ++q4) {
+        double acc[12];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        double acc[kR / 2 * 3];
-#pragma unroll
-        for (int rr = 0; rr < kR / 2; ++rr) {
-            const int r = h * (kR / 2) + rr;
-            const int s = g.s0 + r;
+        for (int t = 0; t < 4; ++t) {
+            const int s = g.s0 + 4 * q4 + t;
             double x = 0.0;
             if (s < n_inner && g.lane_ok) {
-                const int i = scan_row(nx, g.pos, s);
-                x = fma(w.fP[r][lane], X, w.fy[r][lane]);
-                fo[(size_t)i * nv + g.j] = x;
-                const double o = fold[r];
+                const double a = cpl * recip_ge1(one_plus + w.coef[4 * q4 + t][3]);
+                X = fma(a, X, w.buf0[4 * q4 + t][lane]);
+                x = X;
+                fo[(size_t)scan_row(nx, g.pos, s) * nv + g.j] = x;
+                const double o = w.buf1[4 * q4 + t][lane];
                 const double df = fabs(x - o);
                 const double ref = nan_max(fabs(x), fabs(o));
                 q1.add(df, abs_tol + tol * ref);
                 q2.add(df, (ref != ref || ref >= abs_tol) ? ref : abs_tol);
                 bad |= !isfinite(x);
             }
-            acc[3 * rr + 0] = x;
-            acc[3 * rr + 1] = x * vj;
-            acc[3 * rr + 2] = x * vj * vj;
+            acc[3 * t + 0] = x;
+            acc[3 * t + 1] = x * vj;
+            acc[3 * t + 2] = x * vj * vj;
         }
-        store_partials(I, g, vt, lane, acc, h);
+        warp_reduce_scatter<4, 3>(acc, lane);
+        if (owner_writes<4>(lane)) {
+            const int s = g.s0 + 4 * q4 + owner_row<4>(lane);
+            if (s < n_inner) {
+                const int k = scan_row(nx, g.pos, s) - 1;
+                double* p = I.part + ((size_t)vt * n_inner + k) * kPartQ;
+                p[0] = acc[0];
+                p[1] = acc[1];
+                p[2] = acc[2];
+            }
+        }
+    }
+
+    // row-block arrival counting (rows x v-tiles); a block whose count
+    // completes is reduced by this warp right away
+    fence_acq_rel();
+    __syncwarp();
+    if (lane == 0) {
+        w.done_rb[0] = -1;
+        w.done_rb[1] = -1;
+        const int s_lo = g.s0, s_hi = (g.s0 + kR < n_inner ? g.s0 + kR : n_inner) - 1;
+        const int k_a = scan_row(nx, g.pos, s_lo) - 1, k_b = scan_row(nx, g.pos, s_hi) - 1;
+        const int k_lo = k_a < k_b ? k_a : k_b, k_hi = k_a < k_b ? k_b : k_a;
+        int nd = 0;
+        for (int rb = k_lo / kR; rb <= k_hi / kR; ++rb) {
+            const int lo = rb * kR > k_lo ? rb * kR : k_lo;
+            const int hi = (rb + 1) * kR - 1 < k_hi ? (rb + 1) * kR - 1 : k_hi;
+            const unsigned add = (unsigned)(hi - lo + 1);
+            const int rows_in_rb = ((rb + 1) * kR < n_inner ? (rb + 1) * kR : n_inner) - rb * kR;
+            const unsigned expect = (unsigned)rows_in_rb * (unsigned)I.nvt;
+            const unsigned prev = atomicAdd(&I.rbcnt[(size_t)m * I.nrb + rb], add);
+            if (prev + add == expect) w.done_rb[nd++] = rb;
+        }
     }
     __syncwarp();
 }
@@ -556,8 +671,8 @@ __device__ __noinline__ void aa_small_solve(int m, double* A, double* x) {
     }
 }
 
-// Last reduction unit of Anderson call m: Gram matrix from the per-unit
-// partials (lane L sums units L, L+32, ...; fixed butterfly across lanes),
+// Last reduction block of Anderson call m: Gram matrix from the per-block
+// partials (lane L sums blocks L, L+32, ...; fixed butterfly across lanes),
 // regularised Cholesky solve, normalisation by the sum, clip
 // (bgk1d_aa_cpu.py:146-168).
 __device__ __noinline__ void aa_finalize(const double* gpart, int nrb, int mh, double reg,
@@ -591,11 +706,11 @@ __device__ __noinline__ void aa_finalize(const double* gpart, int nrb, int mh, d
     }
 }
 
-// ---- R(m): row reduction / W update, one warp per 32 rows -----------------
-__device__ void reduce_wunit(WarpSmem& w, int ru, int m) {
+// ---- row reduction / W update of one row block (lane = row) -------------
+__device__ __noinline__ void reduce_block(WarpSmem& w, int ru, int m) {
     const ImpInst& I = w.I;
     const int lane = threadIdx.x & 31;
-    const int k = ru * kRW + lane;
+    const int k = ru * kR + lane;
     const bool ok = k < I.n_inner;
     const int i = k + 1;
     const int nx = I.nx, n_inner = I.n_inner, d = 3 * n_inner;
@@ -687,14 +802,14 @@ __device__ void reduce_wunit(WarpSmem& w, int ru, int m) {
                         if (lane == 0) I.gpart[(size_t)ru * kMaxPairs + pi] = v;
                     }
                 }
+            fence_acq_rel();
+            __syncwarp();
             unsigned prev = 0;
-            if (lane == 0) {
-                fence_acq_rel();
-                prev = atomicAdd(&I.rbdone[m], 1u);
-            }
+            if (lane == 0) prev = atomicAdd(&I.rbdone[m], 1u);
             prev = __shfl_sync(0xffffffffu, prev, 0);
             if (prev == (unsigned)I.nrb - 1) {
                 fence_acq_rel();
+                __syncwarp();
                 aa_finalize(I.gpart, I.nrb, mh, I.aa_reg, I.aa_alpha_max,
                             I.alpha + (size_t)m * kMaxAACols);
             }
@@ -713,13 +828,14 @@ __device__ void reduce_wunit(WarpSmem& w, int ru, int m) {
         reinterpret_cast<double2*>(&I.Wc[4 * (size_t)i])[1] = make_double2(c4[2], c4[3]);
     }
     if (ru == 0 && lane == 0) I.st[m] = 1;
+    __syncwarp();
 }
 
-// ---- P2: W^(0) from the moment partials of f^n (one warp per 32 rows) -----
-__device__ void init_wunit(WarpSmem& w, int ru) {
+// ---- P2: W^(0) from the moment partials of f^n (lane = row) --------------
+__device__ void init_block(WarpSmem& w, int ru) {
     const ImpInst& I = w.I;
     const int lane = threadIdx.x & 31;
-    const int k = ru * kRW + lane;
+    const int k = ru * kR + lane;
     const int nx = I.nx, n_inner = I.n_inner;
     if (k < n_inner) {
         double s0, s1, s2;
@@ -756,20 +872,36 @@ __device__ __forceinline__ void flush_residual(const ImpInst& I, int m, FracMax&
     bad = false;
 }
 
+// Phase trace (off unless a buffer is attached): per Picard iteration the
+// earliest start and latest end over all warps of pass 1 and pass 2, in
+// %globaltimer nanoseconds: [m][0] min start p1, [1] max end p1, [2] min start
+// p2, [3] max end p2; row kTraceRows-1 holds the prologue.
+constexpr int kTracePhases = 4;
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void trace_mark(const PlanDev& P, int m, int ph, bool is_min) {
+    if (P.trace == nullptr || (threadIdx.x & 31) != 0 || m >= P.trace_iters) return;
+    unsigned long long* slot = P.trace + (size_t)m * kTracePhases + ph;
+    const unsigned long long t = gtimer();
+    if (is_min) atomicMin(slot, t); else atomicMax(slot, t);
+}
+
 // ---- the persistent kernel --------------------------------------------------
-// Work items (warp-tiles, reduction units) are statically strided over all
-// resident warps of the cooperative grid.  Within an instance, warp-tiles are
-// numbered chunk-major (t = c*nvt + vt) and every warp visits its items in
-// increasing order, so the tile a look-back waits for has a smaller number
-// and is processed by a warp that never waits on a larger one: every wait
-// completes.
-__global__ void __launch_bounds__(kThreads, 2)
+// Work items (warp-tiles, row blocks) are statically strided over all
+// resident warps of the cooperative grid.  Inside a phase no warp waits for
+// another: pass 1 and pass 2 are separated by a grid barrier, and the column
+// scans and row reductions are done by whichever warp completes a column or a
+// row block (arrival counters).
+__global__ void __launch_bounds__(kThreads, 3)
 implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     PlanDev& P = *Pp;
     const unsigned G = gridDim.x;
     const int n_inst = P.n_inst;
-    const long long total_tiles = P.total_tiles, total_ru = P.total_rb;
+    const long long total_tiles = P.total_tiles, total_rb = P.total_rb;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     WarpSmem& w = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
     const long long gwarp = (long long)blockIdx.x * kWarps + warp, nwarps = (long long)G * kWarps;
@@ -787,7 +919,10 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
             I.nonfin[q] = 0;
             I.rbdone[q] = 0u;
         }
-        for (int q = threadIdx.x; q < I.nvt * I.nchunks; q += kThreads) I.lbflag[q] = 0u;
+        for (int q = threadIdx.x; q < I.picard_iter * I.nvt * ((I.nchunks + kGroup - 1) / kGroup);
+             q += kThreads)
+            I.grpcnt[q] = 0u;
+        for (int q = threadIdx.x; q < I.picard_iter * I.nrb; q += kThreads) I.rbcnt[q] = 0u;
         for (int q = threadIdx.x; q < I.nv; q += kThreads) {
             fo[q] = fn[q];
             fo[(size_t)(I.nx - 1) * I.nv + q] = fn[(size_t)(I.nx - 1) * I.nv + q];
@@ -822,10 +957,10 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
     if (!grid_sync(&P.bar, G, &P.err)) return;
 
     // P2: W^(0) (unfloored C1 moments) and coefficients
-    for (long long u = gwarp; u < total_ru; u += nwarps) {
+    for (long long u = gwarp; u < total_rb; u += nwarps) {
         const int b = find_inst(P.rb_off, n_inst, u);
         stage_warp(w, &P.inst[b], b);
-        init_wunit(w, (int)(u - w.I.rb_off));
+        init_block(w, (int)(u - w.I.rb_off));
     }
     if (!grid_sync(&P.bar, G, &P.err)) return;
 
@@ -835,7 +970,22 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
         for (int b = 0; b < n_inst && !any; ++b) any = inst_active(P.inst[b], m);
         if (!any) break;
 
-        // S(m)
+        // pass 1: tile maps and group maps
+        trace_mark(P, m, 0, true);
+        for (long long t = gwarp; t < total_tiles; t += nwarps) {
+            const int b = find_inst(P.tile_off, n_inst, t);
+            stage_warp(w, &P.inst[b], b);
+            if (!inst_active(w.I, m)) continue;
+            const long long tl = t - w.I.tile_off;
+            const int c = (int)(tl / w.I.nvt), vt = (int)(tl % w.I.nvt);
+            map_wtile(w, vt, c, m, swap_io ? w.I.f_out : w.I.f_in);
+        }
+        trace_mark(P, m, 1, false);
+        if (!grid_sync(&P.bar, G, &P.err)) return;
+        trace_mark(P, m, 2, true);
+
+        // pass 2: solve, residual, partial moments; completed row blocks are
+        // reduced on the spot (W update, Anderson history and Gram matrix)
         FracMax q1, q2;
         bool bad = false;
         int res_b = -1;
@@ -849,18 +999,17 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
             const int c = (int)(tl / w.I.nvt), vt = (int)(tl % w.I.nvt);
             const double* fn = swap_io ? w.I.f_out : w.I.f_in;
             double* fo = swap_io ? const_cast<double*>(w.I.f_in) : w.I.f_out;
-            solve_wtile(&P.err, w, vt, c, m, fn, fo, q1, q2, bad);
+            solve_wtile(w, vt, c, m, fn, fo, q1, q2, bad);
+            const int d0 = w.done_rb[0], d1 = w.done_rb[1];
+            if (d0 >= 0 || d1 >= 0) {
+                fence_acq_rel();
+                __syncwarp();
+                if (d0 >= 0) reduce_block(w, d0, m);
+                if (d1 >= 0) reduce_block(w, d1, m);
+            }
         }
         if (res_b >= 0 && inst_active(w.I, m)) flush_residual(w.I, m, q1, q2, bad);
-        if (!grid_sync(&P.bar, G, &P.err)) return;
-
-        // R(m)
-        for (long long u = gwarp; u < total_ru; u += nwarps) {
-            const int b = find_inst(P.rb_off, n_inst, u);
-            stage_warp(w, &P.inst[b], b);
-            if (!inst_active(w.I, m)) continue;
-            reduce_wunit(w, (int)(u - w.I.rb_off), m);
-        }
+        trace_mark(P, m, 3, false);
         if (!grid_sync(&P.bar, G, &P.err)) return;
     }
 
@@ -931,7 +1080,7 @@ Derived derive(int nx, int nv, int kp, const keq_implicit_params& p) {
     d.nt_pos = (nv - kp + 31) / 32;
     d.nvt = d.nt_neg + d.nt_pos;
     d.nchunks = (d.n_inner + keq::kR - 1) / keq::kR;
-    d.nrb = (d.n_inner + keq::kRW - 1) / keq::kRW;
+    d.nrb = (d.n_inner + keq::kR - 1) / keq::kR;
     const int aa_m = p.aa_m > 0 ? p.aa_m : 0;
     d.aa_on = (p.aa_enable && aa_m >= 1 && aa_m + 1 >= 2) ? 1 : 0;
     d.aa_cols = d.aa_on ? aa_m + 1 : 1;
@@ -950,8 +1099,12 @@ size_t carve_instance(void* base, int nx, int nv, int kp, const keq_implicit_par
     double* Wc = c.take<double>(4 * (size_t)nx);
     double* Wb = c.take<double>(8);
     double* part = c.take<double>((size_t)d.nvt * d.n_inner * keq::kPartQ);
-    double* lb = c.take<double>((size_t)d.nvt * d.nchunks * 96);
-    unsigned* lbflag = c.take<unsigned>((size_t)d.nvt * d.nchunks);
+    const int ngroups = (d.nchunks + keq::kGroup - 1) / keq::kGroup;
+    double* agg = c.take<double>((size_t)d.nvt * d.nchunks * 64);
+    double* gmap = c.take<double>((size_t)d.nvt * ngroups * 64);
+    double* crhs = c.take<double>((size_t)nx * nv);
+    unsigned* grpcnt = c.take<unsigned>((size_t)it * d.nvt * ngroups);
+    unsigned* rbcnt = c.take<unsigned>((size_t)it * d.nrb);
     double* res = c.take<double>(2 * (size_t)it);
     int* st = c.take<int>(it);
     int* nonfin = c.take<int>(it);
@@ -961,8 +1114,8 @@ size_t carve_instance(void* base, int nx, int nv, int kp, const keq_implicit_par
     double* alpha = c.take<double>((size_t)it * keq::kMaxAACols);
     unsigned* rbdone = c.take<unsigned>(it);
     if (I) {
-        I->W = W; I->Wn = Wn; I->Wc = Wc; I->Wb = Wb; I->part = part; I->lb = lb;
-        I->lbflag = lbflag; I->res = res; I->st = st; I->nonfin = nonfin; I->aaG = aaG;
+        I->W = W; I->Wn = Wn; I->Wc = Wc; I->Wb = Wb; I->part = part; I->agg = agg;
+        I->gmap = gmap; I->crhs = crhs; I->grpcnt = grpcnt; I->rbcnt = rbcnt; I->res = res; I->st = st; I->nonfin = nonfin; I->aaG = aaG;
         I->aaR = aaR; I->gpart = gpart; I->alpha = alpha; I->rbdone = rbdone;
     }
     return align_up(c.off, 256);
@@ -1239,6 +1392,23 @@ keq_status keq_plan_step(keq_plan* plan, int32_t n_steps, int32_t parity, keq_st
 }
 
 void keq_plan_destroy(keq_plan* plan) { delete plan; }
+
+keq_status keq_plan_set_trace(keq_plan* plan, unsigned long long* trace, int32_t iters,
+                              keq_stream_t stream) {
+    if (!plan || iters < 0 || (iters > 0 && !trace)) return KEQ_ERR_INVALID;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    keq::PlanDev* d = plan->dev;
+    unsigned long long* tp = iters > 0 ? trace : nullptr;
+    cudaError_t e = cudaMemcpyAsync(&d->trace, &tp, sizeof(tp), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&d->trace_iters, &iters, sizeof(int), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        keq_internal_set_cuda_error(e);
+        return KEQ_ERR_CUDA;
+    }
+    return KEQ_OK;
+}
 
 keq_status keq_plan_error(keq_plan* plan, keq_stream_t stream, int32_t* err_bits) {
     if (!plan || !err_bits) return KEQ_ERR_INVALID;

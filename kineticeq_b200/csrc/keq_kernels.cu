@@ -183,6 +183,14 @@ __global__ void __launch_bounds__(64) block_thomas_kernel(const double* __restri
     }
 }
 
+// Evaluates the device math helpers on an array (numerical self-test).
+__global__ void math_selftest_kernel(int kind, const double* __restrict__ x, double* __restrict__ y,
+                                     int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    y[i] = kind == 0 ? exp_nonpos(x[i]) : recip_ge1(x[i]);
+}
+
 }  // namespace keq
 
 namespace {
@@ -221,6 +229,15 @@ keq_status keq_build_system_from_moments(const double* B0, const double* v, int3
     const int blocks = (int)((total + 255) / 256);
     keq::build_system_kernel<<<blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         B0, v, n, nu, T, f_bc_l, f_bc_r, nx, nv, dt, dx, tau_tilde, inv_sqrt_2pi, dl, dd, du, B);
+    return launch_status();
+}
+
+keq_status keq_math_selftest(int32_t kind, const double* x, double* y, int32_t n,
+                             keq_stream_t stream) {
+    if (!x || !y || n < 0 || (kind != 0 && kind != 1)) return KEQ_ERR_INVALID;
+    if (n == 0) return KEQ_OK;
+    keq::math_selftest_kernel<<<(n + 255) / 256, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        kind, x, y, n);
     return launch_status();
 }
 

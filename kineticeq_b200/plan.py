@@ -150,6 +150,33 @@ class ImplicitPlan:
         s = self.specs[i]
         return s.b if self.parity == 0 else s.a
 
+    def enable_trace(self, iters: int = 256) -> torch.Tensor:
+        """Attach a phase trace buffer (see keq_plan_set_trace); returns it."""
+        buf = torch.zeros((iters, 4), dtype=torch.int64, device=self.device)
+        buf[:, 0] = -1  # all ones = UINT64_MAX
+        buf[:, 2] = -1
+        N.check(self._lib.keq_plan_set_trace(self._h, buf.data_ptr(), iters,
+                                             N.stream_handle(self._stream)), "trace")
+        self._trace = buf
+        return buf
+
+    def trace_phases(self):
+        """Per-iteration (pass1_us, barrier_us, pass2_us) of the last step."""
+        import numpy as np
+
+        t = self._trace.cpu().numpy().view(np.uint64).astype(np.float64)
+        out = []
+        for row in t:
+            if row[1] == 0:
+                break
+            out.append(((row[1] - row[0]) / 1e3, (row[2] - row[1]) / 1e3, (row[3] - row[2]) / 1e3))
+        return out
+
+    def reset_trace(self) -> None:
+        self._trace.zero_()
+        self._trace[:, 0] = -1
+        self._trace[:, 2] = -1
+
     def device_error_bits(self) -> int:
         v = C.c_int32(0)
         N.check(self._lib.keq_plan_error(self._h, N.stream_handle(self._stream), C.byref(v)),
