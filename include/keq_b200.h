@@ -161,9 +161,21 @@ keq_status keq_plan_step(keq_plan* plan, int32_t n_steps, int32_t parity, keq_st
  * all warps.  No reference counterpart (profiling aid). */
 keq_status keq_plan_set_trace(keq_plan* plan, unsigned long long* trace, int32_t iters,
                               keq_stream_t stream);
-/* Device-side error bits of the plan (1 << keq_status), synchronising the
- * stream; 0 when every device-side wait completed. */
+/* Device-side error bits of the plan (1 << keq_status) accumulated over every
+ * launch since plan creation or the last keq_plan_reset, synchronising the
+ * stream; 0 when every device-side wait completed.  A launch whose wait gave
+ * up also leaves KEQ_ERR_TIMEOUT in every instance's keq_step_stats.status. */
 keq_status keq_plan_error(keq_plan* plan, keq_stream_t stream, int32_t* err_bits);
+/* Clear the plan's accumulated error bits (asynchronous on the stream).  The
+ * per-launch barrier state is cleared by keq_plan_step itself before every
+ * launch, so a plan stays usable after a launch that timed out.  No reference
+ * counterpart (device-side waits do not exist in the reference). */
+keq_status keq_plan_reset(keq_plan* plan, keq_stream_t stream);
+/* Polls a device-side wait makes before it gives up with KEQ_ERR_TIMEOUT
+ * (default 2^25, i.e. seconds).  0 makes every wait that is not already
+ * satisfied give up at once; tests use it to exercise the timeout path
+ * without a hang.  Synchronises the stream.  No reference counterpart. */
+keq_status keq_plan_set_spin_limit(keq_plan* plan, unsigned long long limit, keq_stream_t stream);
 void keq_plan_destroy(keq_plan* plan);
 
 /* Single-instance convenience wrapper: workspace = instance workspace followed
@@ -210,6 +222,20 @@ keq_status keq_block_tridiag_solve(const double* A, const double* B, const doubl
                                    const double* D, double* X, int32_t n, int32_t batch,
                                    void* workspace, size_t workspace_bytes,
                                    keq_stream_t stream);
+
+/* Maxwellian of per-row moments: core/schemes/BGK1D1V/bgk1d_utils/general/
+ * bgk1d_maxwellian.py:7-33 (maxwellian; used by set_initial_condition,
+ * bgk1d_set_initial_condition.py:9-44): f[i, j] = n_i / sqrt(2 pi T_i)
+ * exp(-(v_j - u_i)^2 / (2 T_i)); n, u, T are (nx), f is (nx, nv). */
+keq_status keq_maxwellian(const double* n, const double* u, const double* T, const double* v,
+                          int32_t nx, int32_t nv, double* f, keq_stream_t stream);
+
+/* Raw row moments without clamps, (nx, 3) row-major: sum f dv, sum f v dv,
+ * sum f v^2/2 dv (the sums of core/schemes/BGK1D1V/bgk1d_utils/general/
+ * bgk1d_compute_moments.py:7-17); the conservation totals of a state are
+ * their sums over x times dx. */
+keq_status keq_row_moments(const double* f, const double* v, int32_t nx, int32_t nv, double dv,
+                           double* out, keq_stream_t stream);
 
 /* Numerical self-test of the device math used by the fused kernels (no
  * reference counterpart): kind 0 evaluates the branch-free e^x for x <= 0,

@@ -86,6 +86,8 @@ _PROTOS = {
     "keq_plan_set_buffers": (_i32, [_vp, C.POINTER(_vp), C.POINTER(_vp), _vp]),
     "keq_plan_step": (_i32, [_vp, _i32, _i32, _vp]),
     "keq_plan_error": (_i32, [_vp, _vp, C.POINTER(_i32)]),
+    "keq_plan_reset": (_i32, [_vp, _vp]),
+    "keq_plan_set_spin_limit": (_i32, [_vp, C.c_uint64, _vp]),
     "keq_plan_set_trace": (_i32, [_vp, _vp, _i32, _vp]),
     "keq_plan_destroy": (None, [_vp]),
     "keq_implicit_workspace_size": (_i32, [C.POINTER(Grid), C.POINTER(ImplicitParams),
@@ -100,6 +102,8 @@ _PROTOS = {
     "keq_block_tridiag_workspace_size": (_i32, [_i32, _i32, C.POINTER(_sz)]),
     "keq_block_tridiag_solve": (_i32, [_dp, _dp, _dp, _dp, _dp, _i32, _i32, _vp, _sz, _vp]),
     "keq_math_selftest": (_i32, [_i32, _dp, _dp, _i32, _vp]),
+    "keq_maxwellian": (_i32, [_dp, _dp, _dp, _dp, _i32, _i32, _dp, _vp]),
+    "keq_row_moments": (_i32, [_dp, _dp, _i32, _i32, _f64, _dp, _vp]),
 }
 
 # Entry points that are declared in the header but may be added by later

@@ -14,8 +14,10 @@ namespace keq {
 constexpr int kLanes = 32;                 // velocities per tile (one warp width)
 constexpr double kTiny = 1.0e-300;         // clamp of n and T in the moment kernels
 constexpr double kInvSqrt2Pi = 0.39894228040143267794;  // 1/sqrt(2 pi), correctly rounded
-// Spin limit of every device-side wait (each poll sleeps ~64-256 ns): a few
-// seconds at most before the wait gives up and reports KEQ_ERR_TIMEOUT.
+// Default spin limit of every device-side wait (each poll sleeps ~32-256 ns):
+// a few seconds at most before the wait gives up and reports KEQ_ERR_TIMEOUT.
+// Plans carry their own copy (keq_plan_set_spin_limit) so that a test can make
+// a wait run out without hanging anything.
 constexpr unsigned long long kSpinLimit = 1ull << 25;
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
@@ -160,7 +162,8 @@ struct GridBarrier {
     unsigned gen;
 };
 
-__device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned nblocks, int* err) {
+__device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned nblocks, int* err,
+                                          unsigned long long limit = kSpinLimit) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -176,7 +179,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned nblocks, int
             unsigned long long it = 0;
             unsigned ns = 32;
             while (ld_acquire(&gb->gen) == g) {
-                if (++it > kSpinLimit) {
+                if (++it > limit) {
                     atomicOr(err, 1 << KEQ_ERR_TIMEOUT);
                     ok = 0;
                     break;
@@ -193,11 +196,12 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned nblocks, int
 }
 
 // Spin (bounded) until *flag >= want.  Returns false on timeout.
-__device__ __forceinline__ bool wait_flag_geq(const unsigned* flag, unsigned want, int* err) {
+__device__ __forceinline__ bool wait_flag_geq(const unsigned* flag, unsigned want, int* err,
+                                              unsigned long long limit = kSpinLimit) {
     unsigned long long it = 0;
     unsigned ns = 16;
     while (ld_acquire(flag) < want) {
-        if (++it > kSpinLimit) {
+        if (++it > limit) {
             atomicOr(err, 1 << KEQ_ERR_TIMEOUT);
             return false;
         }

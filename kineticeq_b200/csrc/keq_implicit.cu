@@ -38,6 +38,7 @@
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
+#include <stddef.h>
 #include <string.h>
 
 #include <vector>
@@ -88,12 +89,18 @@ struct ImpInst {
     unsigned* rbdone;// picard_iter
 };
 
+// Device header of a plan.  The first 16 bytes ({bar, err, err_sticky}) are
+// the launch state: keq_plan_step clears bar and err before every launch, so
+// a launch that gave up on a wait (and left the barrier count behind) cannot
+// poison the next one; err_sticky accumulates the error bits of all launches
+// until keq_plan_reset.
 struct PlanDev {
     GridBarrier bar;
     int err;
+    int err_sticky;
+    unsigned long long spin_limit;
     int n_inst;
     int max_iter;
-    int pad;
     long long total_tiles;
     long long total_rb;
     ImpInst* inst;
@@ -889,6 +896,14 @@ __device__ __forceinline__ void trace_mark(const PlanDev& P, int m, int ph, bool
     if (is_min) atomicMin(slot, t); else atomicMax(slot, t);
 }
 
+// Grid barrier of a launch; on a timeout the error is also recorded in the
+// sticky word read by keq_plan_error.
+__device__ __forceinline__ bool plan_sync(PlanDev& P, unsigned G) {
+    if (grid_sync(&P.bar, G, &P.err, P.spin_limit)) return true;
+    if (threadIdx.x == 0) atomicOr(&P.err_sticky, 1 << KEQ_ERR_TIMEOUT);
+    return false;
+}
+
 // ---- the persistent kernel --------------------------------------------------
 // Work items (warp-tiles, row blocks) are statically strided over all
 // resident warps of the cooperative grid.  Inside a phase no warp waits for
@@ -913,6 +928,9 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
         const ImpInst& I = P.inst[b];
         const double* fn = swap_io ? I.f_out : I.f_in;
         double* fo = swap_io ? const_cast<double*>(I.f_in) : I.f_out;
+        // pending status: stays KEQ_ERR_TIMEOUT unless stage E of this launch
+        // runs, i.e. when a device-side wait gave up and the CTAs returned
+        if (threadIdx.x == 0) I.stats->status = KEQ_ERR_TIMEOUT;
         for (int q = threadIdx.x; q < 2 * I.picard_iter; q += kThreads) I.res[q] = 0.0;
         for (int q = threadIdx.x; q < I.picard_iter; q += kThreads) {
             I.st[q] = 0;
@@ -944,7 +962,7 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
             I.Wb[3 * threadIdx.x + 2] = T;
         }
     }
-    if (!grid_sync(&P.bar, G, &P.err)) return;
+    if (!plan_sync(P, G)) return;
 
     // P1: moments of f^n
     for (long long t = gwarp; t < total_tiles; t += nwarps) {
@@ -954,7 +972,7 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
         const int c = (int)(tl / w.I.nvt), vt = (int)(tl % w.I.nvt);
         moments_wtile(w.I, vt, c, swap_io ? w.I.f_out : w.I.f_in);
     }
-    if (!grid_sync(&P.bar, G, &P.err)) return;
+    if (!plan_sync(P, G)) return;
 
     // P2: W^(0) (unfloored C1 moments) and coefficients
     for (long long u = gwarp; u < total_rb; u += nwarps) {
@@ -962,7 +980,7 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
         stage_warp(w, &P.inst[b], b);
         init_block(w, (int)(u - w.I.rb_off));
     }
-    if (!grid_sync(&P.bar, G, &P.err)) return;
+    if (!plan_sync(P, G)) return;
 
     // Picard iterations
     for (int m = 0; m < P.max_iter; ++m) {
@@ -981,7 +999,7 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
             map_wtile(w, vt, c, m, swap_io ? w.I.f_out : w.I.f_in);
         }
         trace_mark(P, m, 1, false);
-        if (!grid_sync(&P.bar, G, &P.err)) return;
+        if (!plan_sync(P, G)) return;
         trace_mark(P, m, 2, true);
 
         // pass 2: solve, residual, partial moments; completed row blocks are
@@ -1010,7 +1028,7 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
         }
         if (res_b >= 0 && inst_active(w.I, m)) flush_residual(w.I, m, q1, q2, bad);
         trace_mark(P, m, 3, false);
-        if (!grid_sync(&P.bar, G, &P.err)) return;
+        if (!plan_sync(P, G)) return;
     }
 
     // E: statistics
@@ -1303,6 +1321,7 @@ keq_status keq_implicit_plan_create(const keq_instance* insts, int32_t n,
     long long* droff = c.take<long long>(n + 1);
     unsigned* tickets = c.take<unsigned>(max_iter + 1);
     PlanDev h{};
+    h.spin_limit = kSpinLimit;
     h.n_inst = n;
     h.max_iter = max_iter;
     h.total_tiles = toff;
@@ -1379,6 +1398,12 @@ keq_status keq_plan_step(keq_plan* plan, int32_t n_steps, int32_t parity, keq_st
     }
     for (int k = 0; k < n_steps; ++k) {
         int swap_io = ((parity + k) & 1);
+        // fresh barrier and error word for this launch (bar.count, bar.gen, err)
+        cudaError_t me = cudaMemsetAsync(plan->dev, 0, offsetof(PlanDev, err_sticky), s);
+        if (me != cudaSuccess) {
+            keq_internal_set_cuda_error(me);
+            return KEQ_ERR_CUDA;
+        }
         void* args[] = {&plan->dev, &swap_io};
         cudaError_t e = cudaLaunchCooperativeKernel((const void*)keq::implicit_step_kernel,
                                                     dim3(plan->grid), dim3(keq::kThreads), args,
@@ -1414,13 +1439,38 @@ keq_status keq_plan_error(keq_plan* plan, keq_stream_t stream, int32_t* err_bits
     if (!plan || !err_bits) return KEQ_ERR_INVALID;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     int v = 0;
-    cudaError_t e = cudaMemcpyAsync(&v, &plan->dev->err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaError_t e =
+        cudaMemcpyAsync(&v, &plan->dev->err_sticky, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         keq_internal_set_cuda_error(e);
         return KEQ_ERR_CUDA;
     }
     *err_bits = v;
+    return KEQ_OK;
+}
+
+keq_status keq_plan_reset(keq_plan* plan, keq_stream_t stream) {
+    if (!plan) return KEQ_ERR_INVALID;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(plan->dev, 0, offsetof(PlanDev, spin_limit), s);
+    if (e != cudaSuccess) {
+        keq_internal_set_cuda_error(e);
+        return KEQ_ERR_CUDA;
+    }
+    return KEQ_OK;
+}
+
+keq_status keq_plan_set_spin_limit(keq_plan* plan, unsigned long long limit, keq_stream_t stream) {
+    if (!plan) return KEQ_ERR_INVALID;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const unsigned long long v = limit == 0ull ? 0ull : limit;
+    cudaError_t e = cudaMemcpyAsync(&plan->dev->spin_limit, &v, sizeof(v), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        keq_internal_set_cuda_error(e);
+        return KEQ_ERR_CUDA;
+    }
     return KEQ_OK;
 }
 

@@ -183,6 +183,58 @@ __global__ void __launch_bounds__(64) block_thomas_kernel(const double* __restri
     }
 }
 
+// ---- Maxwellian of per-row moments -----------------------------------------
+// bgk1d_utils/general/bgk1d_maxwellian.py:7-33, element for element:
+// coeff = n/sqrt(2 pi T) (n * inv_sqrt_2pi / sqrt(T)), e = (v-u)^2 * (-0.5/T),
+// f = exp(e) * coeff.  One thread per (i, j), j fastest (coalesced rows).
+__global__ void __launch_bounds__(256) maxwellian_kernel(const double* __restrict__ n,
+                                                         const double* __restrict__ u,
+                                                         const double* __restrict__ T,
+                                                         const double* __restrict__ v, int nx,
+                                                         int nv, double* __restrict__ f) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)nx * nv) return;
+    const int i = (int)(t / nv), j = (int)(t % nv);
+    const double Ti = T[i];
+    const double coeff = (n[i] * kInvSqrt2Pi) / sqrt(Ti);
+    const double invT = 0.5 / Ti;
+    const double d = v[j] - u[i];
+    f[t] = exp((d * d) * (-invT)) * coeff;
+}
+
+// ---- raw velocity moments (no clamps) ---------------------------------------
+// Row densities of mass, momentum and energy: (sum f dv, sum f v dv,
+// sum f v^2/2 dv), one warp per row, fixed butterfly order.  Used for the
+// conservation totals of a state and as calculate_moments' raw sums
+// (bgk1d_utils/general/bgk1d_compute_moments.py:7-17).
+__global__ void __launch_bounds__(256) row_moments_kernel(const double* __restrict__ f,
+                                                          const double* __restrict__ v, int nx,
+                                                          int nv, double dv,
+                                                          double* __restrict__ out) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= nx) return;
+    const double* row = f + (size_t)warp * nv;
+    double p0 = 0.0, p1 = 0.0, p2 = 0.0;
+    for (int j = lane; j < nv; j += 32) {
+        const double x = row[j], vj = v[j];
+        p0 += x;
+        p1 += x * vj;
+        p2 += x * (vj * vj);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        p0 += __shfl_xor_sync(0xffffffffu, p0, o);
+        p1 += __shfl_xor_sync(0xffffffffu, p1, o);
+        p2 += __shfl_xor_sync(0xffffffffu, p2, o);
+    }
+    if (lane == 0) {
+        out[3 * (size_t)warp + 0] = p0 * dv;
+        out[3 * (size_t)warp + 1] = p1 * dv;
+        out[3 * (size_t)warp + 2] = 0.5 * (p2 * dv);
+    }
+}
+
 // Evaluates the device math helpers on an array (numerical self-test).
 __global__ void math_selftest_kernel(int kind, const double* __restrict__ x, double* __restrict__ y,
                                      int n) {
@@ -229,6 +281,24 @@ keq_status keq_build_system_from_moments(const double* B0, const double* v, int3
     const int blocks = (int)((total + 255) / 256);
     keq::build_system_kernel<<<blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         B0, v, n, nu, T, f_bc_l, f_bc_r, nx, nv, dt, dx, tau_tilde, inv_sqrt_2pi, dl, dd, du, B);
+    return launch_status();
+}
+
+keq_status keq_maxwellian(const double* n, const double* u, const double* T, const double* v,
+                          int32_t nx, int32_t nv, double* f, keq_stream_t stream) {
+    if (!n || !u || !T || !v || !f || nx < 1 || nv < 1) return KEQ_ERR_INVALID;
+    const long long total = (long long)nx * nv;
+    keq::maxwellian_kernel<<<(unsigned)((total + 255) / 256), 256, 0,
+                             reinterpret_cast<cudaStream_t>(stream)>>>(n, u, T, v, nx, nv, f);
+    return launch_status();
+}
+
+keq_status keq_row_moments(const double* f, const double* v, int32_t nx, int32_t nv, double dv,
+                           double* out, keq_stream_t stream) {
+    if (!f || !v || !out || nx < 1 || nv < 1) return KEQ_ERR_INVALID;
+    const long long threads = (long long)nx * 32;
+    keq::row_moments_kernel<<<(unsigned)((threads + 255) / 256), 256, 0,
+                              reinterpret_cast<cudaStream_t>(stream)>>>(f, v, nx, nv, dv, out);
     return launch_status();
 }
 

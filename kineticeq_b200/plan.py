@@ -84,6 +84,56 @@ class LazyStats:
         return raw.view(_STATS_DTYPE)[: self._n].copy()
 
 
+class StatsRing:
+    """Per-step snapshots of the stats records without a host synchronisation
+    per step: ``capture()`` queues an asynchronous copy of the device records
+    into the next slot of a pinned host ring and returns a ``StatsSnapshot``
+    that waits for that copy only when it is read.  A snapshot read after the
+    ring has wrapped around (``slots`` later captures) raises instead of
+    returning another step's values."""
+
+    def __init__(self, dev: torch.Tensor, n: int, slots: int = 256):
+        self._dev = dev
+        self._n = n
+        self._slots = slots
+        self._host = torch.empty((slots,) + tuple(dev.shape), dtype=dev.dtype, pin_memory=True)
+        self._events = [None] * slots
+        self._gen = [0] * slots
+        self._next = 0
+        self._count = 0
+
+    def capture(self, stream=None) -> "StatsSnapshot":
+        k = self._next
+        self._next = (k + 1) % self._slots
+        self._count += 1
+        s = stream if stream is not None else torch.cuda.current_stream(self._dev.device)
+        with torch.cuda.stream(s):
+            self._host[k].copy_(self._dev, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(s)
+        self._events[k] = ev
+        self._gen[k] = self._count
+        return StatsSnapshot(self, k, self._count)
+
+    def read(self, k: int, gen: int) -> np.ndarray:
+        if self._gen[k] != gen:
+            raise RuntimeError("stats snapshot expired: the ring was reused by later steps")
+        self._events[k].synchronize()
+        raw = np.ascontiguousarray(self._host[k].numpy()).reshape(-1)
+        return raw.view(_STATS_DTYPE)[: self._n].copy()
+
+
+class StatsSnapshot:
+    def __init__(self, ring: StatsRing, k: int, gen: int):
+        self._ring, self._k, self._gen = ring, k, gen
+        self._vals = None
+
+    def fetch(self) -> np.ndarray:
+        if self._vals is None:
+            self._vals = self._ring.read(self._k, self._gen)
+        return self._vals
+
+
 class ImplicitPlan:
     """Batched implicit Picard stepping of independent instances."""
 
@@ -136,11 +186,28 @@ class ImplicitPlan:
         self._lib = lib
         self.parity = 0  # 0: newest state in `a`, 1: in `b`
         self.stats = LazyStats(self.stats_dev, self.n)
+        self._ring = None
 
     def step(self, n_steps: int = 1) -> None:
         N.check(self._lib.keq_plan_step(self._h, int(n_steps), int(self.parity),
                                         N.stream_handle(self._stream)), "implicit step")
         self.parity = (self.parity + int(n_steps)) & 1
+
+    def snapshot(self) -> StatsSnapshot:
+        """Snapshot of the stats records after the steps queued so far."""
+        if self._ring is None:
+            self._ring = StatsRing(self.stats_dev, self.n)
+        return self._ring.capture(self._stream)
+
+    def reset_errors(self) -> None:
+        """Clear the accumulated device error bits (keq_plan_reset)."""
+        N.check(self._lib.keq_plan_reset(self._h, N.stream_handle(self._stream)), "plan reset")
+
+    def set_spin_limit(self, limit: int) -> None:
+        """Polls a device-side wait makes before giving up (keq_plan_set_spin_limit)."""
+        N.check(self._lib.keq_plan_set_spin_limit(self._h, int(limit),
+                                                  N.stream_handle(self._stream)),
+                "spin limit")
 
     def state(self, i: int) -> torch.Tensor:
         s = self.specs[i]

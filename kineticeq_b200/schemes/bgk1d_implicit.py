@@ -27,14 +27,16 @@ Stepper = Callable[[int], None]
 
 
 class LazyBenchlog(Mapping):
-    """benchlog dict whose values are read from the device on first access."""
+    """benchlog dict of one step: a snapshot of the step's device stats record,
+    copied asynchronously when the step is queued and read (with one wait) on
+    first access, so reading it later still gives that step's values."""
 
-    def __init__(self, plan, idx: int, keys: dict):
-        self._plan, self._idx, self._keys, self._vals = plan, idx, keys, None
+    def __init__(self, snap, idx: int, keys: dict):
+        self._snap, self._idx, self._keys, self._vals = snap, idx, keys, None
 
     def _load(self):
         if self._vals is None:
-            rec = self._plan.stats.fetch()[self._idx]
+            rec = self._snap.fetch()[self._idx]
             self._vals = {k: (int(rec[f]) if f in ("iters", "lo_iters", "aa_applied")
                               else float(rec[f])) for k, f in self._keys.items()}
         return self._vals
@@ -109,7 +111,7 @@ def build_stepper(cfg, state) -> Stepper:
             if int(rec["status"]) == N.KEQ_ERR_NONFINITE:
                 raise ValueError("NaN/Inf detected in f_tmp")
             N.check(int(rec["status"]), "implicit step")
-        _stepper.benchlog = LazyBenchlog(plan, 0, IMPLICIT_KEYS)
+        _stepper.benchlog = LazyBenchlog(plan.snapshot(), 0, IMPLICIT_KEYS)
 
     _stepper.benchlog = None
     _stepper.ws = ws
