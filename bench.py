@@ -51,8 +51,33 @@ WORKLOADS = {
     "implicit-8192x1024-aa5-tau1e-4": (8192, 1024, 1e-5, 1e-4,
                                        dict(picard_iter=64, picard_tol=1e-10, abs_tol=1e-16,
                                             aa_enable=True, aa_m=5), 200),
+    "implicit-8192x1024-tau1e-4": (8192, 1024, 1e-5, 1e-4,
+                                   dict(picard_iter=64, picard_tol=1e-10, abs_tol=1e-16), 200),
+    "holo-4096x512-tau5e-5": (4096, 512, 1e-5, 5e-5,
+                              dict(scheme="holo", ho_iter=64, ho_tol=1e-10, lo_iter=64,
+                                   lo_tol=1e-10), 200),
+    "holo-4096x512-tau5e-3": (4096, 512, 1e-5, 5e-3,
+                              dict(scheme="holo", ho_iter=64, ho_tol=1e-10, lo_iter=64,
+                                   lo_tol=1e-10), 200),
+    "holo-256x128-tau5e-5": (256, 128, 5e-6, 5e-5,
+                             dict(scheme="holo", ho_iter=64, ho_tol=1e-10, lo_iter=64,
+                                  lo_tol=1e-10), 100),
+    "holo-8192x1024-tau1e-4": (8192, 1024, 1e-5, 1e-4,
+                               dict(scheme="holo", ho_iter=64, ho_tol=1e-10, lo_iter=64,
+                                    lo_tol=1e-10), 200),
 }
+
+
+def is_holo(name: str) -> bool:
+    return WORKLOADS[name][4].get("scheme") == "holo"
+
+
+def scheme_params(name: str) -> dict:
+    return {k: v for k, v in WORKLOADS[name][4].items() if k != "scheme"}
 DEFAULT_WORKLOAD = "implicit-4096x512-aa5-tau5e-5"
+# Sod initial state (the InitialCondition1D defaults of the reference)
+SOD_REGIONS = ({"x_range": (0.0, 0.5), "n": 1.0, "u": 0.0, "T": 1.0},
+               {"x_range": (0.5, 1.0), "n": 0.125, "u": 0.0, "T": 0.8})
 METRIC = "cell-velocity updates/s"
 BYTES_PER_CELL_ITER = 24  # read f^n, read f^(m), write f^(m+1) (FP64)
 
@@ -161,21 +186,22 @@ def _barrier(dist):
 def make_instance(name: str):
     import torch
 
-    from kineticeq_b200.plan import ImplicitPlan, InstanceSpec, implicit_params_struct
-    from kineticeq_b200.schemes.common import maxwellian
+    from kineticeq_b200.plan import (HoloPlan, ImplicitPlan, InstanceSpec, holo_params_struct,
+                                     implicit_params_struct)
+    from kineticeq_b200.schemes.common import maxwellian, region_moments
     from kineticeq_b200.state import allocate_state_1d1v
 
-    nx, nv, dt, tau, sp, _ = WORKLOADS[name]
+    nx, nv, dt, tau, _, _ = WORKLOADS[name]
+    sp = scheme_params(name)
     st = allocate_state_1d1v(nx, nv, 1.0, 10.0, "cuda", torch.float64)
-    # Sod initial state (BGK1D1V_params.py:26-30 defaults)
-    x = st.x
-    st.n = torch.where(x < 0.5, 1.0, 0.125).to(torch.float64)
-    st.u = torch.zeros_like(x)
-    st.T = torch.where(x < 0.5, 1.0, 0.8).to(torch.float64)
-    st.f.copy_(maxwellian(st))
+    st.n, st.u, st.T = region_moments(st.x, SOD_REGIONS)
+    maxwellian(st, out=st.f)
     spec = InstanceSpec(v=st.v, dx=st.dx, dv=st.dv, dt=dt, tau_tilde=tau, a=st.f,
                         b=torch.empty_like(st.f))
-    plan = ImplicitPlan([spec], implicit_params_struct(**sp))
+    if is_holo(name):
+        plan = HoloPlan([spec], holo_params_struct(**sp))
+    else:
+        plan = ImplicitPlan([spec], implicit_params_struct(**sp))
     return plan, st
 
 
@@ -185,7 +211,9 @@ def run_ours(args, dist, rank, world):
     from kineticeq_b200 import _native as N
 
     name = args.workload
-    nx, nv, dt, tau, sp, case_steps = WORKLOADS[name]
+    nx, nv, dt, tau, _, case_steps = WORKLOADS[name]
+    sp = scheme_params(name)
+    holo = is_holo(name)
     plan, st = make_instance(name)
     f0 = st.f.clone()
     stream = torch.cuda.current_stream()
@@ -216,6 +244,11 @@ def run_ours(args, dist, rank, world):
     if int(rec["status"]) != 0:
         raise RuntimeError(f"device status {N.status_text(int(rec['status']))}")
     iters = int(rec["total_iters"]) - iters0
+    # conservation drift over the timed steps (row moments on the device)
+    from kineticeq_b200.schemes.common import conservation_totals, drift
+
+    drift_k = drift(conservation_totals(plan.state(0), st.v, st.dx, st.dv),
+                    conservation_totals(f0, st.v, st.dx, st.dv))
     ms_max = _max_over_ranks(dist, ms)
     cells = nx * nv
     value = world * cells * args.steps / (ms_max / 1e3)
@@ -244,16 +277,17 @@ def run_ours(args, dist, rank, world):
         e2e = {"value": world * cells * ksteps / (e2e_ms / 1e3), "unit": METRIC,
                "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb}
 
-    # roofline of the step kernel (one launch per step)
+    # roofline of the step kernel (one launch per step): 24 B per cell and
+    # Picard (HO) iteration, plus 16 B per cell and step for HOLO's explicit term
     peak, peak_kind = _peaks()
-    bytes_per_launch = BYTES_PER_CELL_ITER * cells * (iters / args.steps)
+    bytes_per_launch = BYTES_PER_CELL_ITER * cells * (iters / args.steps) + (16 * cells if holo else 0)
     achieved = bytes_per_launch / (ms / args.steps / 1e3) / 1e9
     tpc, tsrc = _traffic_from_profiles(name)
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
             "traffic": (round(tpc * cells * iters / args.steps) if tpc else None),
             "traffic_source": tsrc, "bytes_per_launch_algorithmic": round(bytes_per_launch),
-            "kernel": "keq::implicit_step_kernel"}
+            "kernel": "keq::holo::holo_step_kernel" if holo else "keq::implicit_step_kernel"}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -265,12 +299,14 @@ def run_ours(args, dist, rank, world):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 5),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (Sod initial state, generated on the device)",
-            "config": {"workload": name, "nx": nx, "nv": nv, "dt": dt, "tau_tilde": tau,
-                       "picard_tol": sp["picard_tol"], "picard_iter": sp["picard_iter"],
-                       "anderson_m": sp.get("aa_m") if sp.get("aa_enable") else 0,
+            "config": {"workload": name, "scheme": "holo" if holo else "implicit", "nx": nx,
+                       "nv": nv, "dt": dt, "tau_tilde": tau, **sp,
                        "instances_per_gpu": 1, "parallelism": f"replicas x{world}",
                        "l2": "flushed (256 MiB write) before every timed step",
-                       "mean_picard_iters_per_step": round(iters / args.steps, 3)},
+                       ("mean_ho_iters_per_step" if holo else "mean_picard_iters_per_step"):
+                           round(iters / args.steps, 3)},
+            "drift": {**{k: float(f"{x:.6e}") for k, x in drift_k.items()},
+                      "over_steps": args.steps, "from": "initial state"},
             "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "gpu_launches": launches,
             "clocks": clk.summary(),
         }
@@ -284,24 +320,28 @@ def cpu_baseline(name, f0, st, budget_s=20.0):
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     from oracle import oracle as O
 
-    nx, nv, dt, tau, sp, _ = WORKLOADS[name]
+    nx, nv, dt, tau, _, _ = WORKLOADS[name]
+    sp = scheme_params(name)
     v = st.v.cpu().numpy()
-    p = O.implicit_params(None, **sp)
+    holo = is_holo(name)
+    p = O.holo_params(None, **sp) if holo else O.implicit_params(None, **sp)
+    step = O.holo_step if holo else O.implicit_step
+    key = "ho_iter" if holo else "picard_iter"
     f = f0.copy()
     O.lib()
     t0 = time.perf_counter()
     steps = iters = 0
     while True:
-        bl = O.implicit_step(f, v, st.dx, st.dv, dt, tau, p)
+        bl = step(f, v, st.dx, st.dv, dt, tau, p)
         steps += 1
-        iters += bl["picard_iter"]
+        iters += bl[key]
         el = time.perf_counter() - t0
         if el >= budget_s or steps >= 200:
             break
     val = nx * nv * steps / el
     return {"value": round(val, 1), "unit": METRIC, "cores": int(os.environ["OMP_NUM_THREADS"]),
-            "kind": "port", "sample": f"first {steps} time steps of {name} ({iters} Picard "
-                                      f"iterations) in {el:.1f} s"}
+            "kind": "port", "sample": f"first {steps} time steps of {name} ({iters} "
+                                      f"{'HO' if holo else 'Picard'} iterations) in {el:.1f} s"}
 
 
 def run_reference(args, dist, rank, world):
@@ -316,25 +356,30 @@ def run_reference(args, dist, rank, world):
     from oracle import oracle as O
 
     name = args.workload
-    nx, nv, dt, tau, sp, _ = WORKLOADS[name]
+    nx, nv, dt, tau, _, _ = WORKLOADS[name]
+    sp = scheme_params(name)
+    holo = is_holo(name)
     g = O.Grid(nx, nv)
     v = g.v()
     f = O.initial_condition(g)
-    p = O.implicit_params(None, **sp)
+    p = O.holo_params(None, **sp) if holo else O.implicit_params(None, **sp)
+    step = O.holo_step if holo else O.implicit_step
+    key = "ho_iter" if holo else "picard_iter"
     # bounded sample: at most ~budget seconds of timed steps
     for _ in range(min(args.warmup, 1)):
-        O.implicit_step(f.copy(), v, g.dx, g.dv, dt, tau, p)
+        step(f.copy(), v, g.dx, g.dv, dt, tau, p)
     t0 = time.perf_counter()
     steps = iters = 0
     while steps < args.steps:
-        bl = O.implicit_step(f, v, g.dx, g.dv, dt, tau, p)
+        bl = step(f, v, g.dx, g.dv, dt, tau, p)
         steps += 1
-        iters += bl["picard_iter"]
+        iters += bl[key]
         if time.perf_counter() - t0 > args.cpu_seconds * 6:
             break
     el = time.perf_counter() - t0
     val = nx * nv * steps / el
-    sample = f"first {steps} time steps of {name} ({iters} Picard iterations), {el:.1f} s"
+    sample = (f"first {steps} time steps of {name} ({iters} {'HO' if holo else 'Picard'} "
+              f"iterations), {el:.1f} s")
     out = {"impl": "reference", "metric": METRIC, "value": round(val, 1), "unit": METRIC,
            "n_gpus": world, "steps": steps, "warmup": min(args.warmup, 1),
            "ms_per_step": round(el * 1e3 / steps, 3), "higher_is_better": True,

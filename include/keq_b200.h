@@ -59,7 +59,10 @@ typedef struct keq_grid {
 /* implicit.Params: params/BGK1D1V/implicit.py:5-37 (CNN warm start excluded).
  * conv_type: 0 = "f" (distribution), 1 = "w" (moments).
  * fixed_iters > 0 replays exactly that many Picard iterations per step (the
- * residual is still computed and reported). */
+ * residual is still computed and reported).
+ * tile_rows: scan positions per tile of the step kernel, 8/16/24/32 (0 = 32);
+ * a tuning knob of this backend (no reference counterpart): results depend
+ * on it at rounding level only. */
 typedef struct keq_implicit_params {
     int32_t picard_iter;
     double picard_tol;
@@ -73,6 +76,7 @@ typedef struct keq_implicit_params {
     double aa_reg;
     double aa_alpha_max;
     int32_t fixed_iters;
+    int32_t tile_rows;
 } keq_implicit_params;
 
 /* holo.Params: params/BGK1D1V/holo.py:5-13 (+ the hidden SVdown flag read at
@@ -178,8 +182,32 @@ keq_status keq_plan_reset(keq_plan* plan, keq_stream_t stream);
 keq_status keq_plan_set_spin_limit(keq_plan* plan, unsigned long long limit, keq_stream_t stream);
 void keq_plan_destroy(keq_plan* plan);
 
+/* ==== HOLO step (replaces core/schemes/BGK1D1V/bgk1d_holo_cuda_kernel.py:
+ *      416-595 step() with theta = 1/2: HO moments, consistency terms,
+ *      explicit term, LO Picard with the 3x3 block-tridiagonal solve of
+ *      cuda_kernel/BGK1D1V/lo_blocktridiag, and the distribution solve) =====
+ * A HOLO plan is a keq_plan too: it is stepped, reset, queried and destroyed
+ * with the keq_plan_* functions above.  Each step fills the instance's
+ * keq_step_stats with iters = ho_iter, residual = ho_residual, std_residual =
+ * std_ho_residual, lo_iters, lo_residual, std_lo_residual and max_YI (the
+ * reference's benchlog).  Supported sizes: nx - 2 <= 15872 interior cells
+ * (the LO interface system is solved in one CTA's shared memory); larger
+ * grids return KEQ_ERR_UNSUPPORTED. */
+keq_status keq_holo_instance_workspace_size(const keq_grid* grid, const keq_holo_params* params,
+                                            size_t* bytes);
+keq_status keq_holo_plan_workspace_size(const keq_instance* insts, int32_t n,
+                                        const keq_holo_params* params, int32_t per_instance_params,
+                                        size_t* bytes);
+keq_status keq_holo_plan_create(const keq_instance* insts, int32_t n, const keq_holo_params* params,
+                                int32_t per_instance_params, void* plan_workspace,
+                                size_t plan_workspace_bytes, keq_stream_t stream,
+                                keq_plan** plan_out);
+
 /* Single-instance convenience wrapper: workspace = instance workspace followed
- * by plan workspace, sized by keq_implicit_workspace_size. */
+ * by plan workspace, sized by keq_implicit_workspace_size.  It builds and
+ * destroys a plan per call, which synchronises the stream (v is read back
+ * to find the sign change) and restarts the stats totals; steppers that run
+ * many steps use a plan. */
 keq_status keq_implicit_workspace_size(const keq_grid* grid, const keq_implicit_params* params,
                                        size_t* bytes);
 keq_status keq_implicit_step(const keq_grid* grid, double dt, double tau_tilde,
@@ -212,6 +240,7 @@ keq_status keq_gtsv_workspace_size(int32_t n, int32_t batch, size_t* bytes);
 keq_status keq_gtsv_strided_inplace(const double* dl, const double* d, const double* du,
                                     double* B, int32_t n, int32_t batch, void* workspace,
                                     size_t workspace_bytes, keq_stream_t stream);
+
 
 /* K5: cuda_kernel/BGK1D1V/lo_blocktridiag/block_tridiag_binding.cpp:25-108
  * (block_tridiag_solve): batch 3x3-block tridiagonal systems of n block rows.

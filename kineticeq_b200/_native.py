@@ -40,7 +40,7 @@ class ImplicitParams(C.Structure):
         ("picard_iter", _i32), ("picard_tol", _f64), ("abs_tol", _f64), ("conv_type", _i32),
         ("aa_enable", _i32), ("aa_m", _i32), ("aa_beta", _f64), ("aa_stride", _i32),
         ("aa_start_iter", _i32), ("aa_reg", _f64), ("aa_alpha_max", _f64),
-        ("fixed_iters", _i32),
+        ("fixed_iters", _i32), ("tile_rows", _i32),
     ]
 
 
@@ -90,6 +90,12 @@ _PROTOS = {
     "keq_plan_set_spin_limit": (_i32, [_vp, C.c_uint64, _vp]),
     "keq_plan_set_trace": (_i32, [_vp, _vp, _i32, _vp]),
     "keq_plan_destroy": (None, [_vp]),
+    "keq_holo_instance_workspace_size": (_i32, [C.POINTER(Grid), C.POINTER(HoloParams),
+                                                C.POINTER(_sz)]),
+    "keq_holo_plan_workspace_size": (_i32, [C.POINTER(Instance), _i32, C.POINTER(HoloParams),
+                                            _i32, C.POINTER(_sz)]),
+    "keq_holo_plan_create": (_i32, [C.POINTER(Instance), _i32, C.POINTER(HoloParams), _i32, _vp,
+                                    _sz, _vp, C.POINTER(_vp)]),
     "keq_implicit_workspace_size": (_i32, [C.POINTER(Grid), C.POINTER(ImplicitParams),
                                            C.POINTER(_sz)]),
     "keq_implicit_step": (_i32, [C.POINTER(Grid), _f64, _f64, C.POINTER(ImplicitParams), _dp,

@@ -195,6 +195,23 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned nblocks, int
     return s_ok != 0;
 }
 
+// Common head of every persistent-kernel plan's device header.  The first
+// 16 bytes ({bar, err, err_sticky}) are the launch state: keq_plan_step
+// clears bar and err before every launch, so a launch that gave up on a wait
+// (and left the barrier count behind) cannot poison the next one;
+// err_sticky accumulates the error bits of all launches until
+// keq_plan_reset.
+struct PlanHead {
+    GridBarrier bar;
+    int err;
+    int err_sticky;
+    unsigned long long spin_limit;
+    unsigned long long seq;     // launch sequence (epochs of look-back flags)
+    unsigned long long* trace;  // optional phase trace (profiling aid)
+    int trace_iters;
+    int pad;
+};
+
 // Spin (bounded) until *flag >= want.  Returns false on timeout.
 __device__ __forceinline__ bool wait_flag_geq(const unsigned* flag, unsigned want, int* err,
                                               unsigned long long limit = kSpinLimit) {

@@ -1,0 +1,1591 @@
+// keq_holo.cu -- BGK1D1V HOLO (high-order / low-order) time step for a batch
+// of independent instances, as ONE persistent cooperative kernel per time
+// step on sm_100a.
+//
+// Replaces core/schemes/BGK1D1V/bgk1d_holo_cuda_kernel.py:416-595 (step, theta
+// fixed at 1/2) and its helpers
+//   _HO_calculate_moments_face     :31-77
+//   _HO_calculate_fluxes_Q         :81-99
+//   _compute_explicit_term         :103-131
+//   _compute_Y_I_terms             :135-227
+//   _LO_calculate_moments_picard   :234-409 with the 3x3 block-tridiagonal
+//                                  solve of cuda_kernel/BGK1D1V/lo_blocktridiag/
+//                                  block_tridiag_kernel.cu:80-258
+//   distribution solve             :526-555 (cuSPARSE gtsv in the reference)
+//
+// Phases of one launch (| = grid barrier):
+//   P0  per-step state; boundary rows of f_out; raw moments of the two
+//       boundary rows                                                    |
+//   P1  velocity-moment partials of f^n (tiles)                           |
+//   P2  row reduction: raw half-range sums R^n, HO-old moments, Maxwellian
+//       coefficients; boundary-row Maxwellian sums                        |
+//   P3  explicit term E = f + (1-theta) dt (upwind streaming + (M-f)/tau)
+//       written for the interior rows, and Maxwellian partials of M_old    |
+//   P4  row reduction: old collision moments I_old                        |
+//   HO iteration z:
+//     A   Maxwellian partials of M(f_z) (compute only), W_m = W_HO        |
+//     LO iteration m (partitioned block-tridiagonal solve):
+//       L1  per chunk of rows: (m = 0: Q, face moments, consistency terms
+//           Y, constant part of the right-hand side) block rows from W_m,
+//           local elimination                                             |
+//       L2  per instance: reduced interface system by block PCR           |
+//       L3  per chunk: recovery, W_full, LO residual                      |
+//     C   distribution solve (look-back tiles, keq_tile.cuh) with E and
+//         the LO Maxwellian, HO residual, moment partials of f_{z+1};
+//         completed row blocks reduce R^{z+1}                              |
+//   E   statistics
+//
+// The LO system's blocks have the structure of the flux Jacobian
+// A = [[0,1,0],[u^2,0,0],[0,0,u]] (bgk1d_holo_cuda_kernel.py:317-331), so the
+// 3x3 block system splits exactly into a 2x2 block system for (n, nu) and a
+// scalar tridiagonal system for U; both are solved here by the partition
+// method (chunks of rows eliminated in parallel, interface unknowns by PCR).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stddef.h>
+#include <string.h>
+
+#include <vector>
+
+#include "keq_common.cuh"
+#include "keq_internal.h"
+#include "keq_tile.cuh"
+
+namespace keq {
+namespace holo {
+
+constexpr int kWarps = 4;
+constexpr int kThreads = kWarps * 32;
+constexpr double kTheta = 0.5;
+constexpr int kMaxLoChunk = 64;     // rows per LO chunk at most
+constexpr int kMaxLoChunks = 248;   // LO chunks per instance at most (PCR in shared memory)
+
+struct HoloInst {
+    int nx, nv, n_inner, kp;
+    int nt_neg, nvt, nchunks, nrb;
+    int rows, lo_len, lo_k, pad0;  // tile rows; LO chunk length and count
+    long long tile_off, rb_off, lo_off;
+    double dx, dv, dt, tau_tilde, dtdx2;  // dtdx2 = dt / (2 dx)
+    int ho_iter, lo_iter, con_terms, flux_cons;
+    int sv_down, fixed_ho, fixed_lo, pad1;
+    double ho_tol, ho_abs_tol, lo_tol, lo_abs_tol;
+    const double* v;
+    const double* f_in;
+    double* f_out;
+    keq_step_stats* stats;
+    // workspace carve
+    double* E;       // nx*nv : explicit term (interior rows)
+    double* part;    // nvt*n_inner*kPartQ : moment / Maxwellian partials
+    double* R;       // nx*8 : raw half-range sums of f_z (v>0: 1,v,v^2,v^3 | v<=0: same)
+    double* Rn;      // nx*8 : same for f^n
+    double* Mco;     // nx*4 : HO-old (u, -0.5/T, n/sqrt(2 pi T), 1/tau)
+    double* Wm;      // nx*3 : LO iterate W_m = (n, nu, U)
+    double* Who;     // nx*3 : W_HO
+    double* Iold;    // nx*3 : old collision moments (1-theta) C_old . w dv
+    double* Ib;      // 8    : boundary-row Maxwellian sums (2 rows x 3) + spare
+    double* Y;       // nx*3 : consistency terms of the current HO iteration
+    double* T1;      // nx*3 : W_HO - dt/2dx (F_HO diff) of the current HO iteration
+    double* lorow;   // n_inner*13 : y(3) | P(2x2) | P_U | Q(2x2) | Q_U per row
+    double* loedge;  // lo_k*18 : last-row blocks of each chunk (A,B,C 2x2, D 2 | U: a,b,c,d)
+    double* xi;      // lo_k*3 : interface unknowns
+    double* Wlo;     // 3*nx : n_lo | u_lo | T_lo of the last LO solve (state.n/u/T)
+    double* agg;     // ntiles*64 : tile maps (distribution pass)
+    double* inc;     // ntiles*32 : tile carries
+    unsigned long long* flag;  // ntiles : look-back flags
+    unsigned* rbcnt; // ho_iter*nrb : row-block arrivals of the distribution pass
+    double* ho_red;  // ho_iter*4 : HO std residual, max |df|, max ref, max |Y|
+    double* lo_hist; // ho_iter*lo_iter*2 : LO max |dW|, std residual
+    int* ho_run;     // ho_iter : 1 if HO iteration z ran
+    int* lo_run;     // ho_iter*lo_iter : 1 if LO iteration m of HO iteration z ran
+    int* nonfin;     // ho_iter : non-finite flag of f_{z+1}
+    double* misc;    // 8 : [0] max |f^n| over the boundary rows, [1] max |Y| of the boundary rows
+};
+
+struct HoloDev {
+    PlanHead head;
+    int n_inst;
+    int max_ho, max_lo;
+    int pad;
+    long long total_tiles, total_rb, total_lo;
+    HoloInst* inst;
+    long long* tile_off;
+    long long* rb_off;
+    long long* lo_off;
+    unsigned* tickets;  // max_ho : tile claims of the distribution pass
+};
+
+struct WarpSmem {
+    HoloInst I;
+    double a[kRmax][33];
+    double o[kRmax][32];
+    double coef[kRmax][4];
+    double vv[32];
+    int cur_b, pad;
+    int done_rb[2];
+};
+
+// LO chunk scratch (per warp, aliasing the tile buffers of WarpSmem).
+struct LoRow {
+    double A[4], B[4], C[4], D[2];  // (n, nu) blocks, row-major 2x2
+    double a, b, c, d;              // U
+    double cu;                      // U: C' of the forward sweep
+};
+
+__device__ __forceinline__ TileGeo inst_tile(const HoloInst& I, int vt, int c, int lane) {
+    return tile_geo(I.nt_neg, I.kp, I.nv, I.n_inner, I.rows, vt, c, lane);
+}
+
+__device__ __forceinline__ void stage_warp(WarpSmem& w, const HoloInst* src, int b) {
+    if (w.cur_b != b) {
+        __syncwarp();
+        const int lane = threadIdx.x & 31;
+        const int* s = reinterpret_cast<const int*>(src);
+        int* d = reinterpret_cast<int*>(&w.I);
+        for (int q = lane; q < (int)(sizeof(HoloInst) / sizeof(int)); q += 32) d[q] = __ldg(s + q);
+        __syncwarp();
+        if (lane == 0) w.cur_b = b;
+    }
+    __syncwarp();
+}
+
+template <int STRIDE>
+__device__ __forceinline__ void stage_rows_h(double (*dst)[STRIDE], const double* __restrict__ src,
+                                             const TileGeo& g, int nx, int nv) {
+    const int lane = threadIdx.x & 31;
+    if (!g.lane_ok) return;
+#pragma unroll 8
+    for (int r = 0; r < g.nrows; ++r)
+        cp_async8(&dst[r][lane], src + (size_t)scan_row(nx, g.pos, g.s0 + r) * nv + g.j);
+}
+
+__device__ __forceinline__ void store_partials_h(WarpSmem& w, const TileGeo& g, int vt) {
+    const HoloInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    if (lane < g.nrows) {
+        double s[4];
+        row_sums4(w.a, w.vv, lane, s);
+        const int k = scan_row(I.nx, g.pos, g.s0 + lane) - 1;
+        double* p = I.part + ((size_t)vt * I.n_inner + k) * kPartQ;
+        reinterpret_cast<double2*>(p)[0] = make_double2(s[0], s[1]);
+        reinterpret_cast<double2*>(p)[1] = make_double2(s[2], s[3]);
+    }
+    __syncwarp();
+}
+
+// calculate_moments (bgk1d_utils/general/bgk1d_compute_moments.py:7-17) from
+// raw half-range sums: n = sum f dv, u = (sum f v dv)/n, T = (sum f v^2 dv)/n - u^2.
+struct Mom {
+    double n, u, T, s1, s2, s3;  // s_k = sum f v^k dv
+};
+__device__ __forceinline__ Mom mom_of(const double* R8, double dv) {
+    Mom m;
+    m.n = (R8[0] + R8[4]) * dv;
+    m.s1 = (R8[1] + R8[5]) * dv;
+    m.s2 = (R8[2] + R8[6]) * dv;
+    m.s3 = (R8[3] + R8[7]) * dv;
+    m.u = m.s1 / m.n;
+    m.T = m.s2 / m.n - m.u * m.u;
+    return m;
+}
+// Q = 1/2 sum (v-u)^3 f dv (_HO_calculate_fluxes_Q, :81-99) by the binomial
+// expansion of the raw moments.
+__device__ __forceinline__ double q_of(const Mom& m) {
+    const double u = m.u;
+    return 0.5 * (m.s3 - 3.0 * u * m.s2 + 3.0 * u * u * m.s1 - u * u * u * m.n);
+}
+
+// ---- P1: moment partials of f^n --------------------------------------------
+__device__ __noinline__ void moments_tile(WarpSmem& w, int vt, int c, const double* __restrict__ f) {
+    const HoloInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const TileGeo g = inst_tile(I, vt, c, lane);
+    stage_rows_h<33>(w.a, f, g, I.nx, I.nv);
+    cp_async_commit();
+    w.vv[lane] = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
+    cp_async_wait_all();
+    if (!g.lane_ok)
+        for (int r = 0; r < g.nrows; ++r) w.a[r][lane] = 0.0;
+    store_partials_h(w, g, vt);
+}
+
+// Raw half-range sums of interior row k (v <= 0 tiles, then v > 0 tiles).
+__device__ __forceinline__ void half_sums(const HoloInst& I, int k, double* R8) {
+    double sn[4], sp[4];
+    sum_partials4(I.part, 0, I.nt_neg, I.n_inner, k, sn);
+    sum_partials4(I.part, I.nt_neg, I.nvt, I.n_inner, k, sp);
+    R8[0] = sp[0]; R8[1] = sp[1]; R8[2] = sp[2]; R8[3] = sp[3];
+    R8[4] = sn[0]; R8[5] = sn[1]; R8[6] = sn[2]; R8[7] = sn[3];
+}
+
+// Maxwellian coefficients of (n, u, T) (bgk1d_maxwellian.py:7-33) and 1/tau.
+__device__ __forceinline__ void mc_of(const Mom& m, double tau_tilde, double* c4) {
+    const double sT = sqrt(m.T);
+    c4[0] = m.u;
+    c4[1] = -(0.5 / m.T);
+    c4[2] = (m.n * kInvSqrt2Pi) / sT;
+    c4[3] = (m.n * sT) / tau_tilde;  // 1/tau, tau = tau_tilde / (n sqrt(T))
+}
+
+// Sum over the velocities of a Maxwellian times (1, v, v^2/2), one warp.
+__device__ __forceinline__ void maxwell_sums_row(const double* v, int nv, const double* c4,
+                                                 double* s3) {
+    const int lane = threadIdx.x & 31;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int j = lane; j < nv; j += 32) {
+        const double vj = __ldg(&v[j]);
+        const double d = vj - c4[0];
+        const double M = c4[2] * exp_nonpos(d * d * c4[1]);
+        a0 += M;
+        a1 += M * vj;
+        a2 += M * vj * vj;
+    }
+    s3[0] = warp_sum(a0);
+    s3[1] = warp_sum(a1);
+    s3[2] = 0.5 * warp_sum(a2);
+}
+
+// ---- P3: explicit term and old-Maxwellian partials (one tile) --------------
+__device__ __noinline__ void explicit_tile(WarpSmem& w, int vt, int c, const double* __restrict__ fn) {
+    const HoloInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const TileGeo g = inst_tile(I, vt, c, lane);
+    const int nx = I.nx, nv = I.nv;
+    stage_rows_h<33>(w.a, fn, g, nx, nv);
+    cp_async_commit();
+    const double vj = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
+    w.vv[lane] = vj;
+    if (lane < g.nrows) {
+        const int i = scan_row(nx, g.pos, g.s0 + lane);
+        const double2 q01 = __ldcg(reinterpret_cast<const double2*>(&I.Mco[4 * (size_t)i]));
+        const double2 q23 = __ldcg(reinterpret_cast<const double2*>(&I.Mco[4 * (size_t)i + 2]));
+        w.coef[lane][0] = q01.x; w.coef[lane][1] = q01.y; w.coef[lane][2] = q23.x;
+        w.coef[lane][3] = q23.y;
+    }
+    // upwind neighbour of scan position s0 (scan position s0-1; the
+    // boundary row for s0 = 0)
+    double prev = 0.0;
+    if (g.lane_ok) {
+        const int ip = g.pos ? scan_row(nx, true, g.s0) - 1 : scan_row(nx, false, g.s0) + 1;
+        prev = __ldg(&fn[(size_t)ip * nv + g.j]);
+    }
+    cp_async_wait_all();
+    __syncwarp();
+    const double vc = (-vj) / I.dx;
+    const double a = (1.0 - kTheta) * I.dt;
+    for (int r = 0; r < g.nrows; ++r) {
+        const double f = g.lane_ok ? w.a[r][lane] : 0.0;
+        const double d = vj - w.coef[r][0];
+        const double M = w.coef[r][2] * exp_nonpos(d * d * w.coef[r][1]);
+        // bgk1d_compute_streaming.py: (f_i - f_{i-1}) (-v/dx) for v > 0,
+        // (f_{i+1} - f_i) (-v/dx) for v <= 0
+        const double st = g.pos ? (f - prev) * vc : (prev - f) * vc;
+        const double col = (M - f) * w.coef[r][3];
+        const double e = f + a * (st + col);
+        if (g.lane_ok) I.E[(size_t)scan_row(nx, g.pos, g.s0 + r) * nv + g.j] = e;
+        prev = f;
+        w.a[r][lane] = g.lane_ok ? M : 0.0;  // Maxwellian partials for I_old
+    }
+    store_partials_h(w, g, vt);
+}
+
+// ---- A: Maxwellian partials of M(f_z) (one tile, no memory traffic) --------
+__device__ __noinline__ void maxwell_tile(WarpSmem& w, int vt, int c) {
+    const HoloInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const TileGeo g = inst_tile(I, vt, c, lane);
+    const double vj = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
+    w.vv[lane] = vj;
+    if (lane < g.nrows) {
+        const int i = scan_row(I.nx, g.pos, g.s0 + lane);
+        const Mom m = mom_of(I.R + 8 * (size_t)i, I.dv);
+        double c4[4];
+        mc_of(m, I.tau_tilde, c4);
+        w.coef[lane][0] = c4[0]; w.coef[lane][1] = c4[1]; w.coef[lane][2] = c4[2];
+    }
+    __syncwarp();
+    for (int r = 0; r < g.nrows; ++r) {
+        const double d = vj - w.coef[r][0];
+        const double M = w.coef[r][2] * exp_nonpos(d * d * w.coef[r][1]);
+        w.a[r][lane] = g.lane_ok ? M : 0.0;
+    }
+    store_partials_h(w, g, vt);
+}
+
+// ---- LO: structured blocks -----------------------------------------------------
+// u*, P* of a cell from W = (n, nu, U) (:293-303): den = n + 1e-30,
+// u = nu/den, T = max(2 (U/den - u^2/2), 1e-30), P = n T.
+__device__ __forceinline__ void star_of(const double* W3, double& us, double& Ps) {
+    const double den = W3[0] + 1e-30;
+    us = W3[1] / den;
+    double Ts = 2.0 * (W3[2] / den - 0.5 * us * us);
+    Ts = (Ts != Ts || Ts >= 1e-30) ? Ts : 1e-30;
+    Ps = W3[0] * Ts;
+}
+
+__device__ __forceinline__ bool inv2(const double* M, double* Mi) {
+    const double det = M[0] * M[3] - M[1] * M[2];
+    if (!(fabs(det) >= 1e-30)) {
+        Mi[0] = Mi[1] = Mi[2] = Mi[3] = 0.0;
+        return false;
+    }
+    const double id = 1.0 / det;
+    Mi[0] = M[3] * id;
+    Mi[1] = -M[1] * id;
+    Mi[2] = -M[2] * id;
+    Mi[3] = M[0] * id;
+    return true;
+}
+__device__ __forceinline__ void mm2(const double* A, const double* B, double* C) {
+    C[0] = A[0] * B[0] + A[1] * B[2];
+    C[1] = A[0] * B[1] + A[1] * B[3];
+    C[2] = A[2] * B[0] + A[3] * B[2];
+    C[3] = A[2] * B[1] + A[3] * B[3];
+}
+__device__ __forceinline__ void mv2(const double* A, const double* x, double* y) {
+    y[0] = A[0] * x[0] + A[1] * x[1];
+    y[1] = A[2] * x[0] + A[3] * x[1];
+}
+__device__ __forceinline__ double rcp_or0(double d) { return fabs(d) >= 1e-30 ? 1.0 / d : 0.0; }
+
+// Block row of interior row k (cell i = k+1) from W_m: faces L (i-1, i) and
+// R (i, i+1); AA = -c4 A_L (0 at k = 0), CC = c4 A_R (0 at the last row),
+// BB = I + c4 (A_R - A_L), DD = ((T1 - c2 (b_R - b_L)) + Y).
+__device__ __forceinline__ void lo_row(const HoloInst& I, int k, LoRow& r) {
+    const int i = k + 1;
+    const double* W = I.Wm;
+    double uL, PL, uC, PC, uR, PR;
+    star_of(W + 3 * (size_t)(i - 1), uL, PL);
+    star_of(W + 3 * (size_t)i, uC, PC);
+    star_of(W + 3 * (size_t)(i + 1), uR, PR);
+    const double uhL = 0.5 * (uL + uC), PhL = 0.5 * (PL + PC);
+    const double uhR = 0.5 * (uC + uR), PhR = 0.5 * (PC + PR);
+    const double c4 = I.dt / (4.0 * I.dx), c2 = I.dt / (2.0 * I.dx);
+    const double aL = (k >= 1) ? 1.0 : 0.0, aR = (k <= I.n_inner - 2) ? 1.0 : 0.0;
+    // A_int = [[0,1,0],[uh^2,0,0],[0,0,uh]]
+    const double uL2 = uhL * uhL, uR2 = uhR * uhR;
+    r.A[0] = 0.0; r.A[1] = aL * (1.0 * (-c4)); r.A[2] = aL * (uL2 * (-c4)); r.A[3] = 0.0;
+    r.C[0] = 0.0; r.C[1] = aR * (1.0 * c4); r.C[2] = aR * (uR2 * c4); r.C[3] = 0.0;
+    r.B[0] = (0.0 - 0.0) * c4 + 1.0;
+    r.B[1] = (1.0 - 1.0) * c4;
+    r.B[2] = (uR2 - uL2) * c4;
+    r.B[3] = (0.0 - 0.0) * c4 + 1.0;
+    r.a = aL * (uhL * (-c4));
+    r.c = aR * (uhR * c4);
+    r.b = (uhR - uhL) * c4 + 1.0;
+    // b_int = (0, Ph, uh Ph)
+    const double bd0 = 0.0 - 0.0, bd1 = PhR - PhL, bd2 = uhR * PhR - uhL * PhL;
+    const double* T1 = I.T1 + 3 * (size_t)i;
+    const double* Y = I.Y + 3 * (size_t)i;
+    r.D[0] = __dadd_rn(__dadd_rn(__ldcg(&T1[0]), __dmul_rn(-c2, bd0)), __ldcg(&Y[0]));
+    r.D[1] = __dadd_rn(__dadd_rn(__ldcg(&T1[1]), __dmul_rn(-c2, bd1)), __ldcg(&Y[1]));
+    r.d = __dadd_rn(__dadd_rn(__ldcg(&T1[2]), __dmul_rn(-c2, bd2)), __ldcg(&Y[2]));
+}
+
+// Constant part of the LO right-hand side and the consistency terms Y of row
+// i for HO iteration z (m = 0), from the raw sums of f_z (rows i-1, i, i+1),
+// the Maxwellian partials of M(f_z) and I_old.  Returns max |Y_i|.
+__device__ __noinline__ double lo_prep_row(const HoloInst& I, int k) {
+    const int i = k + 1, nx = I.nx;
+    const double dv = I.dv, dt = I.dt, dx = I.dx;
+    const double c2 = dt / (2.0 * dx);
+    Mom m3[3];
+    double Q3[3];
+    double Rr[3][8];
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        const double* src = I.R + 8 * (size_t)(i - 1 + t);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) Rr[t][q] = __ldcg(&src[q]);
+        m3[t] = mom_of(Rr[t], dv);
+        Q3[t] = q_of(m3[t]);
+    }
+    // face moments S(f) of faces f = i-1 (L) and i (R) (_HO_calculate_moments_face):
+    // upwind state: v > 0 from the left cell, v <= 0 from the right cell
+    double S[2][3];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        const double* Lr = Rr[s];
+        const double* Rg = Rr[s + 1];
+        if (I.sv_down) {
+            S[s][0] = (Lr[0] + Rg[4]) * dv;
+            S[s][1] = (Lr[1] + Rg[5]) * dv;
+            S[s][2] = 0.5 * ((Lr[2] + Rg[6]) * dv);
+        } else {
+            S[s][0] = (Lr[1] + Rg[5]) * dv;
+            S[s][1] = (Lr[2] + Rg[6]) * dv;
+            S[s][2] = 0.5 * ((Lr[3] + Rg[7]) * dv);
+        }
+    }
+    double y[3] = {0.0, 0.0, 0.0};
+    if (I.con_terms) {
+        if (I.flux_cons) {
+            double g[2][3];
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                const Mom& a0 = m3[s];
+                const Mom& a1 = m3[s + 1];
+                const double P0 = a0.n * a0.T, P1 = a1.n * a1.T;
+                const double nu0 = a0.n * a0.u, nu1 = a1.n * a1.u;
+                const double U0 = 0.5 * a0.n * (a0.u * a0.u + a0.T);
+                const double U1 = 0.5 * a1.n * (a1.u * a1.u + a1.T);
+                const double mf0 = nu0 * nu0 / (a0.n + 1e-30) + P0;
+                const double mf1 = nu1 * nu1 / (a1.n + 1e-30) + P1;
+                const double ef0 = (U0 + P0) * a0.u + Q3[s];
+                const double ef1 = (U1 + P1) * a1.u + Q3[s + 1];
+                g[s][0] = -S[s][0] + 0.5 * (nu0 + nu1);
+                g[s][1] = -S[s][1] + 0.5 * (mf0 + mf1);
+                g[s][2] = -S[s][2] + 0.5 * (ef0 + ef1);
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) y[c] = dt * ((g[1][c] - g[0][c]) / dx);
+        }
+        // collision consistency: theta C_new + (1-theta) C_old moments
+        double sM[4];
+        sum_partials4(I.part, 0, I.nvt, I.n_inner, k, sM);
+        const Mom& mn = m3[1];
+        const double inv_tau_new = (mn.n * sqrt(mn.T)) / I.tau_tilde;
+        const double smw[3] = {sM[0] * dv, sM[1] * dv, 0.5 * (sM[2] * dv)};
+        const double sfw[3] = {mn.n, mn.s1, 0.5 * mn.s2};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double cm = kTheta * ((smw[c] - sfw[c]) * inv_tau_new) + __ldcg(&I.Iold[3 * (size_t)i + c]);
+            y[c] = y[c] + dt * cm;
+        }
+    }
+    // constant part of DD: W_HO - dt/2dx (F_HO(R) - F_HO(L)), F_HO = [S1, S2, S3 + 2 Q_half]
+    const double QhL = 0.5 * (Q3[0] + Q3[1]), QhR = 0.5 * (Q3[1] + Q3[2]);
+    const double Fd[3] = {S[1][0] - S[0][0], S[1][1] - S[0][1],
+                          (S[1][2] + 2.0 * QhR) - (S[0][2] + 2.0 * QhL)};
+    double mx = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        I.T1[3 * (size_t)i + c] = __dadd_rn(__ldcg(&I.Who[3 * (size_t)i + c]), __dmul_rn(-c2, Fd[c]));
+        I.Y[3 * (size_t)i + c] = y[c];
+        mx = nan_max(mx, fabs(y[c]));
+    }
+    (void)nx;
+    return mx;
+}
+
+// L1: block rows of one LO chunk into shared memory (lane-parallel), local
+// elimination of rows s..e-1 (lane 0: (n, nu) 2x2 blocks, lane 1: U), and
+// the representation x_i = y_i + P_i xi_{k-1} + Q_i xi_k of every row of the
+// chunk (last row: y = 0, P = 0, Q = I) into lorow; the chunk's last block
+// row into loedge.
+__device__ __noinline__ void lo_chunk_eliminate(WarpSmem& w, int kc) {
+    const HoloInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const int s = kc * I.lo_len;
+    const int e = (s + I.lo_len < I.n_inner ? s + I.lo_len : I.n_inner) - 1;
+    const int len = e - s + 1;
+    LoRow* rows = reinterpret_cast<LoRow*>(&w.a[0][0]);  // kMaxLoChunk rows fit in w.a + w.o
+    for (int r = lane; r < len; r += 32) lo_row(I, s + r, rows[r]);
+    __syncwarp();
+    // last block row of the chunk -> loedge
+    if (lane < 18) {
+        const LoRow& L = rows[len - 1];
+        const double vals[18] = {L.A[0], L.A[1], L.A[2], L.A[3], L.B[0], L.B[1], L.B[2], L.B[3],
+                                 L.C[0], L.C[1], L.C[2], L.C[3], L.D[0], L.D[1],
+                                 L.a, L.b, L.c, L.d};
+        I.loedge[(size_t)kc * 18 + lane] = vals[lane];
+    }
+    // per-row outputs, staged in the o/coef area after the row blocks
+    double* outp = reinterpret_cast<double*>(&rows[kMaxLoChunk]);  // 13 per row
+    const int nloc = len - 1;  // rows s..e-1 eliminated locally
+    if (lane == 0 && nloc > 0) {
+        // forward sweep with C' and R' = [y | P (2 cols) | Q (2 cols)] stored per row
+        double Cp[4], Ry[2], RP[4], RQ[4];
+        for (int r = 0; r < nloc; ++r) {
+            const LoRow& L = rows[r];
+            double M[4], ry[2], rP[4], rQ[4];
+            if (r == 0) {
+                M[0] = L.B[0]; M[1] = L.B[1]; M[2] = L.B[2]; M[3] = L.B[3];
+                ry[0] = L.D[0]; ry[1] = L.D[1];
+                rP[0] = -L.A[0]; rP[1] = -L.A[1]; rP[2] = -L.A[2]; rP[3] = -L.A[3];
+                rQ[0] = rQ[1] = rQ[2] = rQ[3] = 0.0;
+            } else {
+                double T4[4], t2[2];
+                mm2(L.A, Cp, T4);
+                M[0] = L.B[0] - T4[0]; M[1] = L.B[1] - T4[1]; M[2] = L.B[2] - T4[2]; M[3] = L.B[3] - T4[3];
+                mv2(L.A, Ry, t2);
+                ry[0] = L.D[0] - t2[0]; ry[1] = L.D[1] - t2[1];
+                mm2(L.A, RP, T4);
+                rP[0] = -T4[0]; rP[1] = -T4[1]; rP[2] = -T4[2]; rP[3] = -T4[3];
+                mm2(L.A, RQ, T4);
+                rQ[0] = -T4[0]; rQ[1] = -T4[1]; rQ[2] = -T4[2]; rQ[3] = -T4[3];
+            }
+            if (r == nloc - 1) {  // coupling to the chunk's last row moves to the RHS
+                rQ[0] -= L.C[0]; rQ[1] -= L.C[1]; rQ[2] -= L.C[2]; rQ[3] -= L.C[3];
+            }
+            double Mi[4];
+            inv2(M, Mi);
+            mv2(Mi, ry, Ry);
+            mm2(Mi, rP, RP);
+            mm2(Mi, rQ, RQ);
+            if (r < nloc - 1) mm2(Mi, L.C, Cp);
+            double* o = outp + 13 * r;
+            o[0] = Ry[0]; o[1] = Ry[1];
+            o[3] = RP[0]; o[4] = RP[1]; o[5] = RP[2]; o[6] = RP[3];
+            o[8] = RQ[0]; o[9] = RQ[1]; o[10] = RQ[2]; o[11] = RQ[3];
+            // keep C'_r for the backward sweep in the row's (now unused) A slot
+            if (r < nloc - 1) {
+                rows[r].A[0] = Cp[0]; rows[r].A[1] = Cp[1]; rows[r].A[2] = Cp[2]; rows[r].A[3] = Cp[3];
+            }
+        }
+        // backward: x_r = R'_r - C'_r x_{r+1}
+        for (int r = nloc - 2; r >= 0; --r) {
+            const double* Cr = rows[r].A;
+            double* o = outp + 13 * r;
+            const double* on = outp + 13 * (r + 1);
+            double t2[2], T4[4];
+            const double yn[2] = {on[0], on[1]};
+            mv2(Cr, yn, t2);
+            o[0] -= t2[0]; o[1] -= t2[1];
+            const double Pn[4] = {on[3], on[4], on[5], on[6]};
+            mm2(Cr, Pn, T4);
+            o[3] -= T4[0]; o[4] -= T4[1]; o[5] -= T4[2]; o[6] -= T4[3];
+            const double Qn[4] = {on[8], on[9], on[10], on[11]};
+            mm2(Cr, Qn, T4);
+            o[8] -= T4[0]; o[9] -= T4[1]; o[10] -= T4[2]; o[11] -= T4[3];
+        }
+    }
+    if (lane == 1 && nloc > 0) {
+        double cp = 0.0, ry = 0.0, rp = 0.0, rq = 0.0;
+        for (int r = 0; r < nloc; ++r) {
+            const LoRow& L = rows[r];
+            double m, y0, p0, q0;
+            if (r == 0) {
+                m = L.b; y0 = L.d; p0 = -L.a; q0 = 0.0;
+            } else {
+                m = L.b - L.a * cp; y0 = L.d - L.a * ry; p0 = -(L.a * rp); q0 = -(L.a * rq);
+            }
+            if (r == nloc - 1) q0 -= L.c;
+            const double mi = rcp_or0(m);
+            ry = mi * y0; rp = mi * p0; rq = mi * q0;
+            double* o = outp + 13 * r;
+            o[2] = ry; o[7] = rp; o[12] = rq;
+            cp = (r < nloc - 1) ? mi * L.c : 0.0;
+            rows[r].cu = cp;
+        }
+        for (int r = nloc - 2; r >= 0; --r) {
+            const double cr = rows[r].cu;
+            double* o = outp + 13 * r;
+            const double* on = outp + 13 * (r + 1);
+            o[2] -= cr * on[2];
+            o[7] -= cr * on[7];
+            o[12] -= cr * on[12];
+        }
+    }
+    __syncwarp();
+    // rows s..e-1: computed; row e: y = 0, P = 0, Q = I
+    for (int r = lane; r < len; r += 32) {
+        double* dst = I.lorow + 13 * (size_t)(s + r);
+        if (r < nloc) {
+            const double* o = outp + 13 * r;
+#pragma unroll
+            for (int q = 0; q < 13; ++q) dst[q] = o[q];
+        } else {
+#pragma unroll
+            for (int q = 0; q < 13; ++q) dst[q] = 0.0;
+            dst[8] = 1.0; dst[11] = 1.0; dst[12] = 1.0;
+        }
+    }
+}
+
+// Representation (y, P, Q) of the row before row `row0` for chunk kc's
+// interface equation: row e-1 of chunk kc if the chunk has 2+ rows, else the
+// previous chunk's interface unknown itself (y = 0, P = I, Q = 0).
+__device__ __forceinline__ void rep_load(const double* lr, double* o13) {
+#pragma unroll
+    for (int q = 0; q < 13; ++q) o13[q] = __ldcg(&lr[q]);
+}
+
+// L2: the reduced system on the K interface unknowns xi_k (last row of every
+// chunk), one CTA per instance, by parallel cyclic reduction in shared memory:
+//   alpha_k xi_{k-1} + beta_k xi_k + gamma_k xi_{k+1} = delta_k,
+//   alpha = A_e P_{e-1}, beta = B_e + A_e Q_{e-1} + C_e P_{s'},
+//   gamma = C_e Q_{s'}, delta = D_e - A_e y_{e-1} - C_e y_{s'}.
+struct Red2 { double al[4], be[4], ga[4], de[2]; };
+struct Red1 { double al, be, ga, de; };
+
+__device__ __noinline__ void lo_reduced_solve(const HoloInst& I, unsigned char* smem) {
+    const int K = I.lo_k;
+    Red2* b2[2] = {reinterpret_cast<Red2*>(smem), reinterpret_cast<Red2*>(smem) + K};
+    Red1* b1[2] = {reinterpret_cast<Red1*>(smem + 2 * sizeof(Red2) * K),
+                   reinterpret_cast<Red1*>(smem + 2 * sizeof(Red2) * K) + K};
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        const int s = k * I.lo_len;
+        const int e = (s + I.lo_len < I.n_inner ? s + I.lo_len : I.n_inner) - 1;
+        double ed[18];
+#pragma unroll
+        for (int q = 0; q < 18; ++q) ed[q] = __ldcg(&I.loedge[(size_t)k * 18 + q]);
+        const double* A = ed; const double* B = ed + 4; const double* C = ed + 8;
+        const double* D = ed + 12;
+        double pm[13], nx_[13];
+        if (e > s) {
+            rep_load(I.lorow + 13 * (size_t)(e - 1), pm);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 13; ++q) pm[q] = 0.0;
+            pm[3] = 1.0; pm[6] = 1.0; pm[7] = 1.0;
+        }
+        const bool has_next = k + 1 < K;
+        if (has_next) {
+            rep_load(I.lorow + 13 * (size_t)(e + 1), nx_);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 13; ++q) nx_[q] = 0.0;
+        }
+        Red2 r2;
+        double T4[4], U4[4], t2[2], u2[2];
+        mm2(A, pm + 3, r2.al);
+        mm2(A, pm + 8, T4);
+        mm2(C, nx_ + 3, U4);
+        for (int q = 0; q < 4; ++q) r2.be[q] = B[q] + T4[q] + U4[q];
+        mm2(C, nx_ + 8, r2.ga);
+        mv2(A, pm, t2);
+        mv2(C, nx_, u2);
+        r2.de[0] = D[0] - t2[0] - u2[0];
+        r2.de[1] = D[1] - t2[1] - u2[1];
+        b2[0][k] = r2;
+        Red1 r1;
+        const double a = ed[14], b = ed[15], c = ed[16], d = ed[17];
+        r1.al = a * pm[7];
+        r1.be = b + a * pm[12] + c * nx_[7];
+        r1.ga = c * nx_[12];
+        r1.de = d - a * pm[2] - c * nx_[2];
+        b1[0][k] = r1;
+    }
+    __syncthreads();
+    int cur = 0;
+    for (int sd = 1; sd < K; sd <<= 1) {
+        for (int k = threadIdx.x; k < K; k += blockDim.x) {
+            const Red2& me = b2[cur][k];
+            Red2 nw = me;
+            if (k - sd >= 0) {
+                const Red2& lo = b2[cur][k - sd];
+                double bi[4], e1[4], T4[4], t2[2];
+                inv2(lo.be, bi);
+                mm2(me.al, bi, e1);
+                mm2(e1, lo.al, T4);
+                for (int q = 0; q < 4; ++q) nw.al[q] = -T4[q];
+                mm2(e1, lo.ga, T4);
+                for (int q = 0; q < 4; ++q) nw.be[q] -= T4[q];
+                mv2(e1, lo.de, t2);
+                nw.de[0] -= t2[0]; nw.de[1] -= t2[1];
+            } else {
+                for (int q = 0; q < 4; ++q) nw.al[q] = 0.0;
+            }
+            if (k + sd < K) {
+                const Red2& hi = b2[cur][k + sd];
+                double bi[4], e2[4], T4[4], t2[2];
+                inv2(hi.be, bi);
+                mm2(me.ga, bi, e2);
+                mm2(e2, hi.ga, T4);
+                for (int q = 0; q < 4; ++q) nw.ga[q] = -T4[q];
+                mm2(e2, hi.al, T4);
+                for (int q = 0; q < 4; ++q) nw.be[q] -= T4[q];
+                mv2(e2, hi.de, t2);
+                nw.de[0] -= t2[0]; nw.de[1] -= t2[1];
+            } else {
+                for (int q = 0; q < 4; ++q) nw.ga[q] = 0.0;
+            }
+            b2[cur ^ 1][k] = nw;
+            const Red1& m1 = b1[cur][k];
+            Red1 n1 = m1;
+            if (k - sd >= 0) {
+                const Red1& lo = b1[cur][k - sd];
+                const double e1 = m1.al * rcp_or0(lo.be);
+                n1.al = -(e1 * lo.al);
+                n1.be -= e1 * lo.ga;
+                n1.de -= e1 * lo.de;
+            } else {
+                n1.al = 0.0;
+            }
+            if (k + sd < K) {
+                const Red1& hi = b1[cur][k + sd];
+                const double e2 = m1.ga * rcp_or0(hi.be);
+                n1.ga = -(e2 * hi.ga);
+                n1.be -= e2 * hi.al;
+                n1.de -= e2 * hi.de;
+            } else {
+                n1.ga = 0.0;
+            }
+            b1[cur ^ 1][k] = n1;
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        const Red2& r = b2[cur][k];
+        double bi[4], x2[2];
+        inv2(r.be, bi);
+        mv2(bi, r.de, x2);
+        I.xi[3 * (size_t)k + 0] = x2[0];
+        I.xi[3 * (size_t)k + 1] = x2[1];
+        I.xi[3 * (size_t)k + 2] = b1[cur][k].de * rcp_or0(b1[cur][k].be);
+    }
+    __syncthreads();
+}
+
+// L3: recovery of chunk kc's rows, W_full, the LO residual (max |dW| and
+// max |dW| / (abs + tol max(|W_full|, |W_m|))) and W_m <- W_full.
+__device__ __noinline__ void lo_chunk_recover(WarpSmem& w, int kc, int z, int m) {
+    const HoloInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const int s = kc * I.lo_len;
+    const int e = (s + I.lo_len < I.n_inner ? s + I.lo_len : I.n_inner) - 1;
+    double xl[3] = {0.0, 0.0, 0.0}, xr[3];
+    if (kc > 0)
+        for (int q = 0; q < 3; ++q) xl[q] = __ldcg(&I.xi[3 * (size_t)(kc - 1) + q]);
+    for (int q = 0; q < 3; ++q) xr[q] = __ldcg(&I.xi[3 * (size_t)kc + q]);
+    double mdf = 0.0;
+    FracMax fm;
+    for (int r = s + lane; r <= e; r += 32) {
+        const double* o = I.lorow + 13 * (size_t)r;
+        double o13[13];
+        rep_load(o, o13);
+        double x[3];
+        x[0] = o13[0] + (o13[3] * xl[0] + o13[4] * xl[1]) + (o13[8] * xr[0] + o13[9] * xr[1]);
+        x[1] = o13[1] + (o13[5] * xl[0] + o13[6] * xl[1]) + (o13[10] * xr[0] + o13[11] * xr[1]);
+        x[2] = o13[2] + o13[7] * xl[2] + o13[12] * xr[2];
+        if (r == e) { x[0] = xr[0]; x[1] = xr[1]; x[2] = xr[2]; }
+        double* Wr = I.Wm + 3 * (size_t)(r + 1);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const double old = __ldcg(&Wr[q]);
+            const double df = fabs(x[q] - old);
+            const double ref = nan_max(fabs(x[q]), fabs(old));
+            mdf = nan_max(mdf, df);
+            fm.add(df, I.lo_abs_tol + I.lo_tol * ref);
+            Wr[q] = x[q];
+        }
+    }
+    const double a = warp_max(mdf), b = warp_max(fm.value());
+    if (lane == 0) {
+        double* h = I.lo_hist + 2 * ((size_t)z * I.lo_iter + m);
+        atomic_max_nonneg(&h[0], a);
+        atomic_max_nonneg(&h[1], b);
+        if (kc == 0) I.lo_run[(size_t)z * I.lo_iter + m] = 1;
+    }
+}
+
+// ---- C: distribution solve over one tile (theta = 1/2) ------------------------
+// x_s = a_s x_{s-1} + c_s with d = 1 + alpha + beta + theta dt / tau_lo,
+// a = alpha/d, c = (E + theta dt M_lo / tau_lo) / d (:526-555).
+__device__ __noinline__ bool dist_tile(WarpSmem& w, int vt, int c, int z, unsigned long long epoch,
+                          unsigned long long limit, const double* __restrict__ fn,
+                          double* __restrict__ fo, FracMax& q1, double& mdf, double& mref,
+                          bool& bad) {
+    const HoloInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const TileGeo g = inst_tile(I, vt, c, lane);
+    const int nx = I.nx, nv = I.nv;
+    const int nr = g.nrows;
+    stage_rows_h<33>(w.a, I.E, g, nx, nv);
+    stage_rows_h<32>(w.o, z > 0 ? fo : fn, g, nx, nv);
+    cp_async_commit();
+    const double vj = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
+    w.vv[lane] = vj;
+    if (lane < nr) {
+        const int i = scan_row(nx, g.pos, g.s0 + lane);
+        const double* W3 = I.Wm + 3 * (size_t)i;
+        const double n = __ldcg(&W3[0]), nu = __ldcg(&W3[1]), U = __ldcg(&W3[2]);
+        // back to (n, u, T, tau) (:393-407)
+        const double den = n + 1e-30;
+        const double u = nu / den;
+        double T = 2.0 * (U / den - 0.5 * u * u);
+        T = (T != T || T >= 1e-30) ? T : 1e-30;
+        const double sT = sqrt(T);
+        const double tau = I.tau_tilde / (n * sT);
+        w.coef[lane][0] = u;
+        w.coef[lane][1] = -(0.5 / T);
+        w.coef[lane][2] = (n * kInvSqrt2Pi) / sT;
+        w.coef[lane][3] = (kTheta * I.dt) / tau;
+        if (vt == 0) {
+            I.Wlo[i] = n;
+            I.Wlo[nx + i] = u;
+            I.Wlo[2 * nx + i] = T;
+        }
+    }
+    cp_async_wait_all();
+    __syncwarp();
+    const double cpl = I.dtdx2 * fabs(vj);
+    const double one_plus = 1.0 + cpl;
+    double P = 1.0, Y = 0.0;
+#pragma unroll 1
+    for (int r0 = 0; r0 < nr; r0 += 8) {
+        double av[8], cv[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const int r = r0 + t < nr ? r0 + t : nr - 1;
+            const double diff = vj - w.coef[r][0];
+            const double dti = w.coef[r][3];
+            const double M = w.coef[r][2] * exp_nonpos(diff * diff * w.coef[r][1]);
+            const double rr = recip_ge1(one_plus + dti);
+            const double ev = g.lane_ok ? w.a[r][lane] : 0.0;
+            cv[t] = fma(dti, M, ev) * rr;
+            av[t] = cpl * rr;
+        }
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            if (r0 + t < nr) {
+                w.a[r0 + t][lane] = cv[t];
+                Y = fma(av[t], Y, cv[t]);
+                P = P * av[t];
+            }
+        }
+    }
+    const size_t tid = (size_t)c * I.nvt + vt;
+    bool ok = true;
+    double X;
+    if (c == 0) {
+        X = g.lane_ok ? __ldg(&fn[(size_t)(g.pos ? 0 : nx - 1) * nv + g.j]) : 0.0;
+    } else {
+        publish_agg(I.agg, I.flag, tid, P, Y, epoch);
+        ok = lookback(I.agg, I.inc, I.flag, I.nvt, vt, c, epoch, limit, X);
+    }
+    if (c + 1 < I.nchunks) publish_inc(I.inc, I.flag, tid, fma(P, X, Y), epoch);
+    const double tol = I.ho_tol, abs_tol = I.ho_abs_tol;
+#pragma unroll 4
+    for (int r = 0; r < nr; ++r) {
+        const double a = cpl * recip_ge1(one_plus + w.coef[r][3]);
+        X = fma(a, X, w.a[r][lane]);
+        const double x = g.lane_ok ? X : 0.0;
+        w.a[r][lane] = x;
+        if (g.lane_ok) {
+            fo[(size_t)scan_row(nx, g.pos, g.s0 + r) * nv + g.j] = x;
+            const double o = w.o[r][lane];
+            const double df = fabs(x - o);
+            const double ref = nan_max(fabs(x), fabs(o));
+            q1.add(df, abs_tol + tol * ref);
+            mdf = nan_max(mdf, df);
+            mref = nan_max(mref, ref);
+            bad |= !isfinite(x);
+        }
+    }
+    store_partials_h(w, g, vt);
+    return ok;
+}
+
+
+// ---- the persistent kernel ----------------------------------------------------
+__device__ __forceinline__ bool holo_sync(HoloDev& P, unsigned G) {
+    if (grid_sync(&P.head.bar, G, &P.head.err, P.head.spin_limit)) return true;
+    if (threadIdx.x == 0) atomicOr(&P.head.err_sticky, 1 << KEQ_ERR_TIMEOUT);
+    return false;
+}
+
+__device__ __forceinline__ bool ho_stop(const HoloInst& I, int z) {
+    if (I.fixed_ho > 0) return z + 1 >= I.fixed_ho;
+    return __ldcg(&I.ho_red[4 * z + 0]) <= 1.0;  // :566
+}
+__device__ __forceinline__ bool ho_active(const HoloInst& I, int z) {
+    if (z >= I.ho_iter) return false;
+    if (z == 0) return true;
+    if (__ldcg(&I.ho_run[z - 1]) != 1) return false;
+    return !ho_stop(I, z - 1);
+}
+__device__ __forceinline__ bool lo_stop(const HoloInst& I, int z, int m) {
+    if (I.fixed_lo > 0) return m + 1 >= I.fixed_lo;
+    return __ldcg(&I.lo_hist[2 * ((size_t)z * I.lo_iter + m) + 1]) < 1.0;  // :389
+}
+__device__ __forceinline__ bool lo_active(const HoloInst& I, int z, int m) {
+    if (!ho_active(I, z) || m >= I.lo_iter) return false;
+    if (m == 0) return true;
+    if (__ldcg(&I.lo_run[(size_t)z * I.lo_iter + m - 1]) != 1) return false;
+    return !lo_stop(I, z, m - 1);
+}
+
+__device__ __forceinline__ long long claim_h(unsigned* tickets, int z) {
+    unsigned t = 0;
+    if ((threadIdx.x & 31) == 0) t = atomicAdd(&tickets[z], 1u);
+    return (long long)__shfl_sync(0xffffffffu, t, 0);
+}
+
+// P2 row reduction (lane = interior row): raw half sums of f^n, HO-old
+// moments, W_HO and the old Maxwellian's coefficients.
+__device__ void init_rows(WarpSmem& w, int ru) {
+    const HoloInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const int k = ru * kRB + lane;
+    if (k >= I.n_inner) return;
+    const int i = k + 1;
+    double R8[8];
+    half_sums(I, k, R8);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        I.Rn[8 * (size_t)i + q] = R8[q];
+        I.R[8 * (size_t)i + q] = R8[q];
+    }
+    const Mom m = mom_of(R8, I.dv);
+    double c4[4];
+    mc_of(m, I.tau_tilde, c4);
+    reinterpret_cast<double2*>(I.Mco + 4 * (size_t)i)[0] = make_double2(c4[0], c4[1]);
+    reinterpret_cast<double2*>(I.Mco + 4 * (size_t)i)[1] = make_double2(c4[2], c4[3]);
+    // W_HO = (n, n u, n (u^2 + T) / 2) (:268-271)
+    I.Who[3 * (size_t)i + 0] = m.n;
+    I.Who[3 * (size_t)i + 1] = m.n * m.u;
+    I.Who[3 * (size_t)i + 2] = 0.5 * m.n * (m.u * m.u + m.T);
+}
+
+// Boundary rows (warp-wide, row ib in {0, nx-1}): raw half sums from P0,
+// W_HO, the Maxwellian sums and the constant consistency term
+// Y_b = dt (sum M w - sum f w) dv / tau (C_new = C_old on these rows).
+__device__ __noinline__ void init_boundary_row(WarpSmem& w, int side) {
+    const HoloInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const int ib = side == 0 ? 0 : I.nx - 1;
+    double R8[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) R8[q] = __ldcg(&I.Rn[8 * (size_t)ib + q]);
+    const Mom m = mom_of(R8, I.dv);
+    double c4[4];
+    mc_of(m, I.tau_tilde, c4);
+    double sm[3];
+    maxwell_sums_row(I.v, I.nv, c4, sm);
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) I.R[8 * (size_t)ib + q] = R8[q];
+        reinterpret_cast<double2*>(I.Mco + 4 * (size_t)ib)[0] = make_double2(c4[0], c4[1]);
+        reinterpret_cast<double2*>(I.Mco + 4 * (size_t)ib)[1] = make_double2(c4[2], c4[3]);
+        I.Who[3 * (size_t)ib + 0] = m.n;
+        I.Who[3 * (size_t)ib + 1] = m.n * m.u;
+        I.Who[3 * (size_t)ib + 2] = 0.5 * m.n * (m.u * m.u + m.T);
+        const double sfw[3] = {m.n, m.s1, 0.5 * m.s2};
+        double mx = 0.0;
+        for (int q = 0; q < 3; ++q) {
+            const double y = I.con_terms ? I.dt * (((sm[q] * I.dv) - sfw[q]) * c4[3]) : 0.0;
+            I.Y[3 * (size_t)ib + q] = y;
+            mx = nan_max(mx, fabs(y));
+        }
+        atomic_max_nonneg(&I.misc[1], mx);
+        // n_lo, u_lo, T_lo of the boundary rows (W_m = W_HO there)
+        const double den = m.n + 1e-30;
+        const double u = (m.n * m.u) / den;
+        double T = 2.0 * ((0.5 * m.n * (m.u * m.u + m.T)) / den - 0.5 * u * u);
+        T = (T != T || T >= 1e-30) ? T : 1e-30;
+        I.Wlo[ib] = m.n;
+        I.Wlo[I.nx + ib] = u;
+        I.Wlo[2 * I.nx + ib] = T;
+    }
+}
+
+// P4 (lane = interior row): I_old = (1-theta) (sum M_old w - sum f^n w) dv / tau_old.
+__device__ void iold_rows(WarpSmem& w, int ru) {
+    const HoloInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const int k = ru * kRB + lane;
+    if (k >= I.n_inner) return;
+    const int i = k + 1;
+    double sM[4], R8[8];
+    sum_partials4(I.part, 0, I.nvt, I.n_inner, k, sM);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) R8[q] = __ldcg(&I.Rn[8 * (size_t)i + q]);
+    const Mom m = mom_of(R8, I.dv);
+    const double inv_tau = __ldcg(&I.Mco[4 * (size_t)i + 3]);
+    const double smw[3] = {sM[0] * I.dv, sM[1] * I.dv, 0.5 * (sM[2] * I.dv)};
+    const double sfw[3] = {m.n, m.s1, 0.5 * m.s2};
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+        I.Iold[3 * (size_t)i + q] = (1.0 - kTheta) * ((smw[q] - sfw[q]) * inv_tau);
+}
+
+// Row reduction after the distribution pass (lane = interior row): raw half
+// sums of f_{z+1}.
+__device__ void ho_rows(WarpSmem& w, int ru, int z) {
+    const HoloInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const int k = ru * kRB + lane;
+    if (k < I.n_inner) {
+        double R8[8];
+        half_sums(I, k, R8);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) I.R[8 * (size_t)(k + 1) + q] = R8[q];
+    }
+    if (ru == 0 && lane == 0) I.ho_run[z] = 1;
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restrict__ Pp,
+                                                                int swap_io) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    HoloDev& P = *Pp;
+    const unsigned G = gridDim.x;
+    const int n_inst = P.n_inst;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    WarpSmem& w = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
+    const long long gwarp = (long long)blockIdx.x * kWarps + warp, nwarps = (long long)G * kWarps;
+    const long long total_tiles = P.total_tiles, total_rb = P.total_rb, total_lo = P.total_lo;
+    if (lane == 0) w.cur_b = -1;
+    __syncwarp();
+
+    // P0
+    if (blockIdx.x == 0) {
+        for (int q = threadIdx.x; q < P.max_ho; q += kThreads) P.tickets[q] = 0u;
+        if (threadIdx.x == 0) P.head.seq = P.head.seq + 1ull;
+    }
+    for (int b = blockIdx.x; b < n_inst; b += G) {
+        const HoloInst& I = P.inst[b];
+        const double* fn = swap_io ? I.f_out : I.f_in;
+        double* fo = swap_io ? const_cast<double*>(I.f_in) : I.f_out;
+        if (threadIdx.x == 0) I.stats->status = KEQ_ERR_TIMEOUT;  // pending until stage E
+        for (int q = threadIdx.x; q < 4 * I.ho_iter; q += kThreads) I.ho_red[q] = 0.0;
+        for (int q = threadIdx.x; q < 2 * I.ho_iter * I.lo_iter; q += kThreads) I.lo_hist[q] = 0.0;
+        for (int q = threadIdx.x; q < I.ho_iter * I.lo_iter; q += kThreads) I.lo_run[q] = 0;
+        for (int q = threadIdx.x; q < I.ho_iter; q += kThreads) {
+            I.ho_run[q] = 0;
+            I.nonfin[q] = 0;
+        }
+        for (int q = threadIdx.x; q < I.ho_iter * I.nrb; q += kThreads) I.rbcnt[q] = 0u;
+        for (int q = threadIdx.x; q < 8; q += kThreads) I.misc[q] = 0.0;
+        for (int q = threadIdx.x; q < I.nv; q += kThreads) {
+            fo[q] = fn[q];
+            fo[(size_t)(I.nx - 1) * I.nv + q] = fn[(size_t)(I.nx - 1) * I.nv + q];
+        }
+        __syncthreads();
+        if (threadIdx.x < 2) {
+            // boundary row raw half sums (sequential) and max |f|
+            const int ib = threadIdx.x == 0 ? 0 : I.nx - 1;
+            const double* row = fn + (size_t)ib * I.nv;
+            double R8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            double mx = 0.0;
+            for (int j = 0; j < I.nv; ++j) {
+                const double x = row[j], vj = I.v[j];
+                const double t1 = x * vj, t2 = t1 * vj;
+                const int o = vj > 0.0 ? 0 : 4;
+                R8[o + 0] += x;
+                R8[o + 1] += t1;
+                R8[o + 2] += t2;
+                R8[o + 3] = fma(t2, vj, R8[o + 3]);
+                mx = nan_max(mx, fabs(x));
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) I.Rn[8 * (size_t)ib + q] = R8[q];
+            atomic_max_nonneg(&I.misc[0], mx);
+        }
+    }
+    if (!holo_sync(P, G)) return;
+    const unsigned long long seq = __ldcg(&P.head.seq);
+    const unsigned long long limit = P.head.spin_limit;
+
+    // P1: moment partials of f^n
+    for (long long t = gwarp; t < total_tiles; t += nwarps) {
+        const int b = find_inst(P.tile_off, n_inst, t);
+        stage_warp(w, &P.inst[b], b);
+        const long long tl = t - w.I.tile_off;
+        moments_tile(w, (int)(tl % w.I.nvt), (int)(tl / w.I.nvt), swap_io ? w.I.f_out : w.I.f_in);
+    }
+    if (!holo_sync(P, G)) return;
+
+    // P2: per-row HO-old data; boundary rows
+    for (long long u = gwarp; u < total_rb; u += nwarps) {
+        const int b = find_inst(P.rb_off, n_inst, u);
+        stage_warp(w, &P.inst[b], b);
+        init_rows(w, (int)(u - w.I.rb_off));
+    }
+    for (long long u = gwarp; u < 2LL * n_inst; u += nwarps) {
+        const int b = (int)(u >> 1);
+        stage_warp(w, &P.inst[b], b);
+        init_boundary_row(w, (int)(u & 1));
+    }
+    if (!holo_sync(P, G)) return;
+
+    // P3: explicit term and old-Maxwellian partials
+    for (long long t = gwarp; t < total_tiles; t += nwarps) {
+        const int b = find_inst(P.tile_off, n_inst, t);
+        stage_warp(w, &P.inst[b], b);
+        const long long tl = t - w.I.tile_off;
+        explicit_tile(w, (int)(tl % w.I.nvt), (int)(tl / w.I.nvt), swap_io ? w.I.f_out : w.I.f_in);
+    }
+    if (!holo_sync(P, G)) return;
+
+    // P4: I_old
+    for (long long u = gwarp; u < total_rb; u += nwarps) {
+        const int b = find_inst(P.rb_off, n_inst, u);
+        stage_warp(w, &P.inst[b], b);
+        iold_rows(w, (int)(u - w.I.rb_off));
+    }
+    if (!holo_sync(P, G)) return;
+
+    for (int z = 0; z < P.max_ho; ++z) {
+        bool any = false;
+        for (int b = 0; b < n_inst && !any; ++b) any = ho_active(P.inst[b], z);
+        if (!any) break;
+
+        // A: Maxwellian partials of M(f_z); W_m = W_HO; boundary |Y| into max_YI
+        for (long long t = gwarp; t < total_tiles; t += nwarps) {
+            const int b = find_inst(P.tile_off, n_inst, t);
+            stage_warp(w, &P.inst[b], b);
+            if (!ho_active(w.I, z) || !w.I.con_terms) continue;
+            const long long tl = t - w.I.tile_off;
+            maxwell_tile(w, (int)(tl % w.I.nvt), (int)(tl / w.I.nvt));
+        }
+        for (int b = blockIdx.x; b < n_inst; b += G) {
+            const HoloInst& I = P.inst[b];
+            if (!ho_active(I, z)) continue;
+            for (int q = threadIdx.x; q < 3 * I.nx; q += kThreads) I.Wm[q] = __ldcg(&I.Who[q]);
+            if (threadIdx.x == 0) atomic_max_nonneg(&I.ho_red[4 * z + 3], __ldcg(&I.misc[1]));
+        }
+        if (!holo_sync(P, G)) return;
+
+        // LO Picard iterations
+        for (int m = 0; m < P.max_lo; ++m) {
+            bool lany = false;
+            for (int b = 0; b < n_inst && !lany; ++b) lany = lo_active(P.inst[b], z, m);
+            if (!lany) break;
+            // L1
+            for (long long u = gwarp; u < total_lo; u += nwarps) {
+                const int b = find_inst(P.lo_off, n_inst, u);
+                stage_warp(w, &P.inst[b], b);
+                if (!lo_active(w.I, z, m)) continue;
+                const int kc = (int)(u - w.I.lo_off);
+                if (m == 0) {
+                    const int s0 = kc * w.I.lo_len;
+                    const int e0 = (s0 + w.I.lo_len < w.I.n_inner ? s0 + w.I.lo_len : w.I.n_inner);
+                    double mx = 0.0;
+                    for (int k = s0 + lane; k < e0; k += 32) mx = nan_max(mx, lo_prep_row(w.I, k));
+                    mx = warp_max(mx);
+                    if (lane == 0) atomic_max_nonneg(&w.I.ho_red[4 * z + 3], mx);
+                    __syncwarp();
+                }
+                lo_chunk_eliminate(w, kc);
+            }
+            if (!holo_sync(P, G)) return;
+            // L2: one CTA per instance
+            if (lane == 0) w.cur_b = -1;  // shared memory is reused below
+            __syncthreads();
+            for (int b = blockIdx.x; b < n_inst; b += G) {
+                const HoloInst& I = P.inst[b];
+                if (!lo_active(I, z, m)) continue;
+                lo_reduced_solve(I, smem_raw);
+            }
+            __syncthreads();
+            if (lane == 0) w.cur_b = -1;
+            __syncwarp();
+            if (!holo_sync(P, G)) return;
+            // L3
+            for (long long u = gwarp; u < total_lo; u += nwarps) {
+                const int b = find_inst(P.lo_off, n_inst, u);
+                stage_warp(w, &P.inst[b], b);
+                if (!lo_active(w.I, z, m)) continue;
+                lo_chunk_recover(w, (int)(u - w.I.lo_off), z, m);
+            }
+            if (!holo_sync(P, G)) return;
+        }
+
+        // C: distribution solve
+        {
+            const unsigned long long epoch = seq * (unsigned long long)(P.max_ho + 1) + z + 1;
+            FracMax q1;
+            double mdf = 0.0, mref = 0.0;
+            bool bad = false;
+            int res_b = -1;
+            for (;;) {
+                const long long t = claim_h(P.tickets, z);
+                if (t >= total_tiles) break;
+                const int b = find_inst(P.tile_off, n_inst, t);
+                if (b != res_b && res_b >= 0 && ho_active(w.I, z)) {
+                    const double r1 = warp_max(q1.value()), r2 = warp_max(mdf), r3 = warp_max(mref);
+                    const bool nb = __any_sync(0xffffffffu, bad);
+                    if (lane == 0) {
+                        atomic_max_nonneg(&w.I.ho_red[4 * z + 0], r1);
+                        atomic_max_nonneg(&w.I.ho_red[4 * z + 1], r2);
+                        atomic_max_nonneg(&w.I.ho_red[4 * z + 2], r3);
+                        if (nb) atomicOr(&w.I.nonfin[z], 1);
+                    }
+                    q1 = FracMax();
+                    mdf = mref = 0.0;
+                    bad = false;
+                }
+                stage_warp(w, &P.inst[b], b);
+                res_b = b;
+                if (!ho_active(w.I, z)) continue;
+                const long long tl = t - w.I.tile_off;
+                const int c = (int)(tl / w.I.nvt), vt = (int)(tl % w.I.nvt);
+                const double* fn = swap_io ? w.I.f_out : w.I.f_in;
+                double* fo = swap_io ? const_cast<double*>(w.I.f_in) : w.I.f_out;
+                if (!dist_tile(w, vt, c, z, epoch, limit, fn, fo, q1, mdf, mref, bad)) {
+                    if (lane == 0) {
+                        atomicOr(&P.head.err, 1 << KEQ_ERR_TIMEOUT);
+                        atomicOr(&P.head.err_sticky, 1 << KEQ_ERR_TIMEOUT);
+                    }
+                }
+                const TileGeo g = inst_tile(w.I, vt, c, lane);
+                fence_acq_rel();
+                __syncwarp();
+                if (lane == 0)
+                    rowblock_arrive(w.I.rbcnt + (size_t)z * w.I.nrb, w.I.nx, w.I.n_inner, w.I.nvt,
+                                    g, w.done_rb);
+                __syncwarp();
+                const int d0 = w.done_rb[0], d1 = w.done_rb[1];
+                if (d0 >= 0 || d1 >= 0) {
+                    fence_acq_rel();
+                    __syncwarp();
+                    if (d0 >= 0) ho_rows(w, d0, z);
+                    if (d1 >= 0) ho_rows(w, d1, z);
+                }
+            }
+            if (res_b >= 0 && ho_active(w.I, z)) {
+                const double r1 = warp_max(q1.value()), r2 = warp_max(mdf), r3 = warp_max(mref);
+                const bool nb = __any_sync(0xffffffffu, bad);
+                if (lane == 0) {
+                    atomic_max_nonneg(&w.I.ho_red[4 * z + 0], r1);
+                    atomic_max_nonneg(&w.I.ho_red[4 * z + 1], r2);
+                    atomic_max_nonneg(&w.I.ho_red[4 * z + 2], r3);
+                    if (nb) atomicOr(&w.I.nonfin[z], 1);
+                }
+            }
+        }
+        if (!holo_sync(P, G)) return;
+    }
+
+    // E: statistics (benchlog keys of :586-594)
+    for (int b = blockIdx.x; b < n_inst; b += G) {
+        if (threadIdx.x != 0) continue;
+        const HoloInst& I = P.inst[b];
+        int last = -1;
+        for (int z = 0; z < I.ho_iter; ++z) {
+            if (__ldcg(&I.ho_run[z]) == 1) last = z;
+            else break;
+        }
+        keq_step_stats* st = I.stats;
+        int status = KEQ_OK;
+        int lo_last = -1;
+        double lo_df = 0.0, lo_std = 0.0, ho_std = 0.0, ho_rel = 0.0, myi = 0.0;
+        if (last >= 0) {
+            for (int m = 0; m < I.lo_iter; ++m) {
+                if (__ldcg(&I.lo_run[(size_t)last * I.lo_iter + m]) == 1) lo_last = m;
+                else break;
+            }
+            if (lo_last >= 0) {
+                lo_df = __ldcg(&I.lo_hist[2 * ((size_t)last * I.lo_iter + lo_last)]);
+                lo_std = __ldcg(&I.lo_hist[2 * ((size_t)last * I.lo_iter + lo_last) + 1]);
+            }
+            ho_std = __ldcg(&I.ho_red[4 * last + 0]);
+            const double mref = nan_max(__ldcg(&I.ho_red[4 * last + 2]), __ldcg(&I.misc[0]));
+            ho_rel = __ldcg(&I.ho_red[4 * last + 1]) / mref;
+            myi = __ldcg(&I.ho_red[4 * last + 3]);
+            if (__ldcg(&I.nonfin[last])) status = KEQ_ERR_NONFINITE;
+        }
+        if (__ldcg(&P.head.err) & (1 << KEQ_ERR_TIMEOUT)) status = KEQ_ERR_TIMEOUT;
+        st->status = status;
+        st->iters = last + 1;
+        st->aa_applied = 0;
+        st->lo_iters = lo_last + 1;
+        st->residual = ho_rel;
+        st->std_residual = ho_std;
+        st->lo_residual = lo_df;
+        st->std_lo_residual = lo_std;
+        st->max_YI = myi;
+        st->total_iters += last + 1;
+        st->total_steps += 1;
+    }
+}
+
+constexpr size_t kSmemBytes = sizeof(WarpSmem) * kWarps;
+static_assert(2 * (sizeof(Red2) + sizeof(Red1)) * kMaxLoChunks <= kSmemBytes,
+              "reduced LO system must fit the CTA's shared memory");
+static_assert(sizeof(LoRow) * kMaxLoChunk + 13 * sizeof(double) * kMaxLoChunk <=
+                  sizeof(WarpSmem) - offsetof(WarpSmem, a),
+              "LO chunk scratch must fit a warp's shared memory");
+
+}  // namespace holo
+}  // namespace keq
+
+// ===========================================================================
+// Host side
+// ===========================================================================
+namespace {
+
+using keq::holo::HoloDev;
+using keq::holo::HoloInst;
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+struct Carve {
+    char* base;
+    size_t off;
+    template <class T>
+    T* take(size_t count) {
+        off = align_up(off, 256);
+        T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+        off += sizeof(T) * (count ? count : 1);
+        return p;
+    }
+};
+
+struct HDerived {
+    int n_inner, nt_neg, nvt, rows, nchunks, nrb, lo_len, lo_k;
+};
+
+HDerived hderive(int nx, int nv, int kp) {
+    HDerived d;
+    d.n_inner = nx - 2;
+    d.nt_neg = (kp + 31) / 32;
+    d.nvt = d.nt_neg + (nv - kp + 31) / 32;
+    d.rows = keq::kRmax;
+    d.nchunks = (d.n_inner + d.rows - 1) / d.rows;
+    d.nrb = (d.n_inner + keq::kRB - 1) / keq::kRB;
+    // LO chunks: multiples of 32 rows, few enough for the reduced system
+    int q = (d.n_inner + 32 * keq::holo::kMaxLoChunks - 1) / (32 * keq::holo::kMaxLoChunks);
+    if (q < 1) q = 1;
+    d.lo_len = 32 * q;
+    d.lo_k = (d.n_inner + d.lo_len - 1) / d.lo_len;
+    return d;
+}
+
+bool holo_valid(const keq_holo_params& p) {
+    return p.ho_iter >= 1 && p.ho_iter <= 4096 && p.lo_iter >= 1 && p.lo_iter <= 4096 &&
+           (long long)p.ho_iter * p.lo_iter <= (1LL << 22);
+}
+
+size_t carve_holo(void* base, int nx, int nv, int kp, const keq_holo_params& p, HoloInst* I) {
+    const HDerived d = hderive(nx, nv, kp);
+    Carve c{static_cast<char*>(base), 0};
+    const size_t ntiles = (size_t)d.nvt * d.nchunks;
+    const size_t ho = (size_t)p.ho_iter, lo = (size_t)p.lo_iter;
+    double* Wlo = c.take<double>(3 * (size_t)nx);  // first: the host reads it as state.n/u/T
+    double* E = c.take<double>((size_t)nx * nv);
+    double* part = c.take<double>((size_t)d.nvt * d.n_inner * keq::kPartQ);
+    double* R = c.take<double>(8 * (size_t)nx);
+    double* Rn = c.take<double>(8 * (size_t)nx);
+    double* Mco = c.take<double>(4 * (size_t)nx);
+    double* Wm = c.take<double>(3 * (size_t)nx);
+    double* Who = c.take<double>(3 * (size_t)nx);
+    double* Iold = c.take<double>(3 * (size_t)nx);
+    double* Ib = c.take<double>(8);
+    double* Y = c.take<double>(3 * (size_t)nx);
+    double* T1 = c.take<double>(3 * (size_t)nx);
+    double* lorow = c.take<double>(13 * (size_t)d.n_inner);
+    double* loedge = c.take<double>(18 * (size_t)d.lo_k);
+    double* xi = c.take<double>(3 * (size_t)d.lo_k);
+    double* agg = c.take<double>(ntiles * 64);
+    double* inc = c.take<double>(ntiles * 32);
+    unsigned long long* flag = c.take<unsigned long long>(ntiles);
+    unsigned* rbcnt = c.take<unsigned>(ho * d.nrb);
+    double* ho_red = c.take<double>(4 * ho);
+    double* lo_hist = c.take<double>(2 * ho * lo);
+    int* ho_run = c.take<int>(ho);
+    int* lo_run = c.take<int>(ho * lo);
+    int* nonfin = c.take<int>(ho);
+    double* misc = c.take<double>(8);
+    if (I) {
+        I->E = E; I->part = part; I->R = R; I->Rn = Rn; I->Mco = Mco; I->Wm = Wm; I->Who = Who;
+        I->Iold = Iold; I->Ib = Ib; I->Y = Y; I->T1 = T1; I->lorow = lorow; I->loedge = loedge;
+        I->xi = xi; I->Wlo = Wlo; I->agg = agg; I->inc = inc; I->flag = flag; I->rbcnt = rbcnt;
+        I->ho_red = ho_red; I->lo_hist = lo_hist; I->ho_run = ho_run; I->lo_run = lo_run;
+        I->nonfin = nonfin; I->misc = misc;
+    }
+    return align_up(c.off, 256);
+}
+
+size_t holo_plan_bytes(int n, int max_ho) {
+    Carve c{nullptr, 0};
+    c.take<HoloDev>(1);
+    c.take<HoloInst>(n);
+    c.take<long long>(n + 1);
+    c.take<long long>(n + 1);
+    c.take<long long>(n + 1);
+    c.take<unsigned>(max_ho + 1);
+    return align_up(c.off, 256);
+}
+
+}  // namespace
+
+extern "C" {
+
+keq_status keq_holo_instance_workspace_size(const keq_grid* grid, const keq_holo_params* params,
+                                            size_t* bytes) {
+    if (!grid || !params || !bytes) return KEQ_ERR_INVALID;
+    if (grid->nx < 3 || grid->nv < 1 || !holo_valid(*params)) return KEQ_ERR_INVALID;
+    size_t best = 0;
+    const int kps[3] = {0, grid->nv, grid->nv / 2 + 1 <= grid->nv ? grid->nv / 2 + 1 : grid->nv};
+    for (int q = 0; q < 3; ++q) {
+        const size_t b = carve_holo(nullptr, grid->nx, grid->nv, kps[q], *params, nullptr);
+        if (b > best) best = b;
+    }
+    const size_t worst =
+        carve_holo(nullptr, grid->nx, grid->nv + 64, (grid->nv + 64) / 2, *params, nullptr);
+    *bytes = worst > best ? worst : best;
+    return KEQ_OK;
+}
+
+keq_status keq_holo_plan_workspace_size(const keq_instance* insts, int32_t n,
+                                        const keq_holo_params* params, int32_t per_instance_params,
+                                        size_t* bytes) {
+    if (!insts || n < 1 || !params || !bytes) return KEQ_ERR_INVALID;
+    int max_ho = 1;
+    for (int b = 0; b < n; ++b) {
+        const int h = params[per_instance_params ? b : 0].ho_iter;
+        if (h > max_ho) max_ho = h;
+    }
+    *bytes = holo_plan_bytes(n, max_ho);
+    return KEQ_OK;
+}
+
+keq_status keq_holo_plan_create(const keq_instance* insts, int32_t n, const keq_holo_params* params,
+                                int32_t per_instance_params, void* plan_ws, size_t plan_ws_bytes,
+                                keq_stream_t stream, keq_plan** plan_out) {
+    using namespace keq;
+    if (!insts || n < 1 || !params || !plan_ws || !plan_out) return KEQ_ERR_INVALID;
+    if (reinterpret_cast<uintptr_t>(plan_ws) % 256) return KEQ_ERR_WORKSPACE;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    int dev_of_buffers = -1;
+    {
+        cudaPointerAttributes pa{};
+        if (cudaPointerGetAttributes(&pa, insts[0].f_in) != cudaSuccess ||
+            pa.type != cudaMemoryTypeDevice) {
+            cudaGetLastError();
+            return KEQ_ERR_INVALID;
+        }
+        dev_of_buffers = pa.device;
+        if (cudaSetDevice(dev_of_buffers) != cudaSuccess) {
+            keq_internal_set_cuda_error(cudaGetLastError());
+            return KEQ_ERR_CUDA;
+        }
+    }
+    int max_ho = 1, max_lo = 1;
+    for (int b = 0; b < n; ++b) {
+        const keq_holo_params& p = params[per_instance_params ? b : 0];
+        if (!holo_valid(p)) return KEQ_ERR_INVALID;
+        if (p.ho_iter > max_ho) max_ho = p.ho_iter;
+        if (p.lo_iter > max_lo) max_lo = p.lo_iter;
+    }
+    if (plan_ws_bytes < holo_plan_bytes(n, max_ho)) return KEQ_ERR_WORKSPACE;
+
+    keq_plan* plan = new keq_plan();
+    plan->kind = KEQ_PLAN_HOLO;
+    plan->n_inst = n;
+    plan->device = dev_of_buffers;
+    plan->inst_bytes = sizeof(HoloInst);
+    plan->off_f_in = offsetof(HoloInst, f_in);
+    plan->off_f_out = offsetof(HoloInst, f_out);
+    plan->kernel = (const void*)holo::holo_step_kernel;
+    plan->smem = holo::kSmemBytes;
+    plan->threads = holo::kThreads;
+    plan->host_inst.resize(sizeof(HoloInst) * (size_t)n);
+    std::vector<HoloInst> host(n);
+    std::vector<long long> toff(n + 1), roff(n + 1), loff(n + 1);
+    long long t = 0, r = 0, l = 0;
+    std::vector<double> vh;
+    cudaError_t e = cudaSuccess;
+    for (int b = 0; b < n; ++b) {
+        const keq_instance& in = insts[b];
+        const keq_holo_params& p = params[per_instance_params ? b : 0];
+        const int nx = in.grid.nx, nv = in.grid.nv;
+        if (nx < 3 || nv < 1 || !in.grid.v || !in.f_in || !in.f_out || !in.stats ||
+            !in.workspace || in.f_in == in.f_out || !(in.dt > 0.0) || !(in.tau_tilde > 0.0) ||
+            !(in.grid.dx > 0.0) || !(in.grid.dv > 0.0)) {
+            delete plan;
+            return KEQ_ERR_INVALID;
+        }
+        if (reinterpret_cast<uintptr_t>(in.workspace) % 256) {
+            delete plan;
+            return KEQ_ERR_WORKSPACE;
+        }
+        vh.resize(nv);
+        if (cudaMemcpyAsync(vh.data(), in.grid.v, sizeof(double) * nv, cudaMemcpyDeviceToHost, s) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
+            keq_internal_set_cuda_error(cudaGetLastError());
+            delete plan;
+            return KEQ_ERR_CUDA;
+        }
+        int kp = 0;
+        for (int j = 0; j < nv; ++j) {
+            if (j > 0 && !(vh[j] > vh[j - 1])) {
+                delete plan;
+                return KEQ_ERR_INVALID;
+            }
+            if (!(vh[j] > 0.0)) kp = j + 1;
+        }
+        const HDerived d = hderive(nx, nv, kp);
+        if (d.lo_len > holo::kMaxLoChunk || d.lo_k > holo::kMaxLoChunks) {
+            delete plan;
+            return KEQ_ERR_UNSUPPORTED;  // nx beyond the LO solver's capacity
+        }
+        HoloInst I{};
+        I.nx = nx; I.nv = nv; I.n_inner = d.n_inner; I.kp = kp;
+        I.nt_neg = d.nt_neg; I.nvt = d.nvt; I.nchunks = d.nchunks; I.nrb = d.nrb;
+        I.rows = d.rows; I.lo_len = d.lo_len; I.lo_k = d.lo_k;
+        I.tile_off = t; I.rb_off = r; I.lo_off = l;
+        I.dx = in.grid.dx; I.dv = in.grid.dv; I.dt = in.dt; I.tau_tilde = in.tau_tilde;
+        I.dtdx2 = in.dt / (2.0 * in.grid.dx);
+        I.ho_iter = p.ho_iter; I.lo_iter = p.lo_iter;
+        I.con_terms = p.con_terms_do ? 1 : 0; I.flux_cons = p.flux_consistency_do ? 1 : 0;
+        I.sv_down = p.sv_down ? 1 : 0; I.fixed_ho = p.fixed_ho_iters; I.fixed_lo = p.fixed_lo_iters;
+        I.ho_tol = p.ho_tol; I.ho_abs_tol = p.ho_abs_tol; I.lo_tol = p.lo_tol;
+        I.lo_abs_tol = p.lo_abs_tol;
+        I.v = in.grid.v; I.f_in = in.f_in; I.f_out = in.f_out; I.stats = in.stats;
+        carve_holo(in.workspace, nx, nv, kp, p, &I);
+        e = cudaMemsetAsync(I.flag, 0, sizeof(unsigned long long) * (size_t)d.nvt * d.nchunks, s);
+        if (e != cudaSuccess) break;
+        host[b] = I;
+        toff[b] = t; roff[b] = r; loff[b] = l;
+        t += (long long)d.nvt * d.nchunks;
+        r += d.nrb;
+        l += d.lo_k;
+    }
+    if (e != cudaSuccess) {
+        keq_internal_set_cuda_error(e);
+        delete plan;
+        return KEQ_ERR_CUDA;
+    }
+    toff[n] = t; roff[n] = r; loff[n] = l;
+    if (t >= (long long)0xffffffffll) {
+        delete plan;
+        return KEQ_ERR_INVALID;
+    }
+    memcpy(plan->host_inst.data(), host.data(), sizeof(HoloInst) * (size_t)n);
+    Carve c{static_cast<char*>(plan_ws), 0};
+    HoloDev* dev = c.take<HoloDev>(1);
+    HoloInst* dinst = c.take<HoloInst>(n);
+    long long* dt_ = c.take<long long>(n + 1);
+    long long* dr_ = c.take<long long>(n + 1);
+    long long* dl_ = c.take<long long>(n + 1);
+    unsigned* tickets = c.take<unsigned>(max_ho + 1);
+    HoloDev h{};
+    h.head.spin_limit = kSpinLimit;
+    h.n_inst = n;
+    h.max_ho = max_ho;
+    h.max_lo = max_lo;
+    h.total_tiles = t;
+    h.total_rb = r;
+    h.total_lo = l;
+    h.inst = dinst;
+    h.tile_off = dt_;
+    h.rb_off = dr_;
+    h.lo_off = dl_;
+    h.tickets = tickets;
+    plan->dev = dev;
+    plan->dev_inst = dinst;
+    e = cudaMemcpyAsync(dev, &h, sizeof(h), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dinst, host.data(), sizeof(HoloInst) * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dt_, toff.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dr_, roff.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dl_, loff.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        for (int b = 0; b < n && e == cudaSuccess; ++b)
+            e = cudaMemsetAsync(insts[b].stats, 0, sizeof(keq_step_stats), s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        keq_internal_set_cuda_error(e);
+        delete plan;
+        return KEQ_ERR_CUDA;
+    }
+    const keq_status gs = keq_internal_plan_grid(plan);
+    if (gs != KEQ_OK) {
+        delete plan;
+        return gs;
+    }
+    *plan_out = plan;
+    return KEQ_OK;
+}
+
+}  // extern "C"

@@ -12,55 +12,58 @@
 //                         (numerics of the CPU twin bgk1d_utils/implicit/bgk1d_aa_cpu.py:7-129)
 //
 // Structure of one launch (one time step for every instance of the plan):
-//   P0  zero per-step device state, copy the fixed boundary rows to f_out
-//   P1  velocity moments of f^n (tile partial sums)          -- grid barrier
-//   P2  row reduction -> W^(0)=(n,nu,T), per-row coefficients -- grid barrier
-//   loop over Picard iterations m while any instance is active:
-//     S(m)  fused tile pass: Maxwellian + upwind implicit assembly + solve of
-//           the first-order recurrence along x (decoupled look-back between
-//           x-chunks), residual vs f^(m), partial moments of f^(m+1)
-//                                                              -- grid barrier
-//     R(m)  row reduction of the partial moments -> W_new, "w" residual,
-//           Anderson history / Gram matrix (last block solves the m x m
-//           system), W^(m+1) and per-row coefficients         -- grid barrier
+//   P0  per-step device state, boundary rows of f_out, boundary-row moments
+//                                                           -- grid barrier
+//   P1  velocity moments of f^n (tile partial sums)         -- grid barrier
+//   P2  row reduction -> W^(0) = (n, nu, T), row coefficients -- grid barrier
+//   per Picard iteration m while any instance is active, ONE pass over the
+//   tiles (claimed in x order from a global ticket):
+//     Maxwellian + upwind implicit assembly of the tile's rows, composition
+//     of the tile map, decoupled look-back for the carry (keq_tile.cuh),
+//     recurrence, write of f^(m+1), residual against f^(m), partial moments;
+//     the warp that completes a row block reduces it: W_new, the "w"
+//     residual, Anderson history and Gram partials (the last row block
+//     solves the small Anderson system)              -- grid barrier
 //   E   per-instance statistics
+//
+// Per cell and Picard iteration the pass reads f^n and f^(m) and writes
+// f^(m+1): 24 bytes in FP64; the Maxwellian, the coefficients and the
+// moments stay on chip.  f_out holds the newest iterate and is updated in
+// place (each element is read as f^(m) and rewritten as f^(m+1) by the same
+// lane).
 //
 // The upwind system of one velocity row is bidiagonal (alpha = dt/dx max(v,0),
 // beta = dt/dx max(-v,0), one of them is zero): for v > 0
 //     x_i = (b_i + alpha x_{i-1}) / d_i,   x_0 = f^n(0, v)      (forward in x)
-// and for v <= 0 the mirror image backward from f^n(nx-1, v).  Velocity tiles
-// are split at the sign change so that a tile scans in one direction only.
-// Each tile of 32 velocities x LX scan positions composes affine maps
-// x -> P x + Y per thread segment, per tile, and between tiles through a
-// deterministic decoupled look-back (predecessor maps are applied in a fixed
-// nested order, so the result does not depend on timing).
+// with d_i = 1 + alpha + dt/tau_i and b_i = f^n_i + dt/tau_i M_i(v), and for
+// v <= 0 the mirror image backward from f^n(nx-1, v).
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stddef.h>
 #include <stdio.h>
 #include <stdlib.h>
-#include <stddef.h>
 #include <string.h>
 
 #include <vector>
 
 #include "keq_common.cuh"
 #include "keq_internal.h"
+#include "keq_tile.cuh"
 
 namespace keq {
 
 constexpr int kWarps = 4;                // warps per CTA
 constexpr int kThreads = kWarps * 32;
-constexpr int kR = 32;                   // rows (scan positions) per warp-tile = rows per row block
 constexpr int kMaxAACols = 8;            // Anderson ring columns (aa_m <= 7)
 constexpr int kMaxPairs = kMaxAACols * (kMaxAACols + 1) / 2;
-constexpr int kPartQ = 4;                // doubles per (v-tile,row) partial
 
 struct ImpInst {
     int nx, nv, n_inner, kp;
     int nt_neg, nvt, nchunks, nrb;
+    int rows, pad0;  // rows per tile (R)
     long long tile_off, rb_off;
     double dx, dv, dt, tau_tilde, dtdx, u_max;
-    int picard_iter, conv_type, fixed_iters;
+    int picard_iter, conv_type, fixed_iters, pad1;
     double tol, abs_tol;
     int aa_on, aa_cols, aa_stride, aa_start;
     double aa_beta, aa_reg, aa_alpha_max;
@@ -74,11 +77,10 @@ struct ImpInst {
     double* Wc;      // 4*nx  : per-row (u, -1/(2T), n/sqrt(2 pi T), dt/tau)
     double* Wb;      // 8     : moments of the two boundary rows
     double* part;    // nvt*n_inner*kPartQ
-    double* agg;     // nvt*nchunks*64 : tile maps (P | Y per lane)
-    double* gmap;    // nvt*ngroups*64 : composed maps of groups of chunks
-    double* crhs;    // nx*nv : scaled right-hand side c = b/d of the current iterate
-    unsigned* grpcnt;// picard_iter*nvt*ngroups : tiles of a chunk group done (pass 1)
-    unsigned* rbcnt; // picard_iter*nrb  : rows x v-tiles of a row block done (pass 2)
+    double* agg;     // ntiles*64 : tile maps (P | Y per lane)
+    double* inc;     // ntiles*32 : tile inclusive values (carry out)
+    unsigned long long* flag;  // ntiles : (epoch << 2) | {agg, inc}
+    unsigned* rbcnt; // picard_iter*nrb  : rows x v-tiles of a row block done
     double* res;     // 2*picard_iter : std / rel residual slots
     int* st;         // picard_iter   : 1 if active in iteration m
     int* nonfin;     // picard_iter   : non-finite flag of iterate m+1
@@ -89,16 +91,9 @@ struct ImpInst {
     unsigned* rbdone;// picard_iter
 };
 
-// Device header of a plan.  The first 16 bytes ({bar, err, err_sticky}) are
-// the launch state: keq_plan_step clears bar and err before every launch, so
-// a launch that gave up on a wait (and left the barrier count behind) cannot
-// poison the next one; err_sticky accumulates the error bits of all launches
-// until keq_plan_reset.
+// Device header of an implicit plan (starts with the common PlanHead).
 struct PlanDev {
-    GridBarrier bar;
-    int err;
-    int err_sticky;
-    unsigned long long spin_limit;
+    PlanHead head;
     int n_inst;
     int max_iter;
     long long total_tiles;
@@ -106,32 +101,19 @@ struct PlanDev {
     ImpInst* inst;
     long long* tile_off;  // n_inst+1
     long long* rb_off;    // n_inst+1
-    unsigned* tickets;    // max_iter+1 (reserved)
-    unsigned long long* trace;  // optional: kTracePhases stamps per iteration (ns)
-    int trace_iters;
+    unsigned* tickets;    // max_iter : tile claims of iteration m
 };
 
 // Per-warp shared memory.
 struct WarpSmem {
     ImpInst I;
-    double buf0[kR][32];   // pass 1: f^n tile; pass 2: c tile
-    double buf1[kR][32];   // pass 2: previous iterate (residual reference)
-    double coef[kR][4];    // (u, -1/(2T), n/sqrt(2 pi T), dt/tau) per row
-    int cur_b;
+    double a[kRmax][33];   // f^n tile -> c = b/d -> x (solution), row stride 33
+    double o[kRmax][32];   // f^(m) tile (residual reference)
+    double coef[kRmax][4]; // (u, -1/(2T), n/sqrt(2 pi T), dt/tau) per row
+    double vv[32];         // the tile's velocities (0 where absent)
+    int cur_b, cur_m, cur_active, pad;
     int done_rb[2];
-    int pad;
 };
-
-__device__ __forceinline__ int find_inst(const long long* off, int n, long long t) {
-    int lo = 0, hi = n;  // off[lo] <= t < off[hi]
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(&off[mid]) <= t) lo = mid; else hi = mid;
-    }
-    return lo;
-}
-
-__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
 __device__ __forceinline__ bool iter_done(const ImpInst& I, int m) {
     // Convergence test of iteration m (bgk1d_implicit_cuda_kernel.py:241).
@@ -190,60 +172,9 @@ __device__ __forceinline__ double clamp_min_t(double x, double lo) {
     return (x != x || x >= lo) ? x : lo;
 }
 
-// Sum of the per-v-tile partial moments of interior row k, in v-tile order
-// (loads issued in batches of 8 so their latencies overlap).
-__device__ __forceinline__ void sum_partials(const double* part, int nvt, int n_inner, int k,
-                                             double* s0, double* s1, double* s2) {
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    for (int v0 = 0; v0 < nvt; v0 += 8) {
-        double2 p01[8];
-        double p2[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            if (v0 + q < nvt) {
-                const double* p = part + ((size_t)(v0 + q) * n_inner + k) * kPartQ;
-                p01[q] = __ldcg(reinterpret_cast<const double2*>(p));
-                p2[q] = __ldcg(p + 2);
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            if (v0 + q < nvt) {
-                a0 += p01[q].x;
-                a1 += p01[q].y;
-                a2 += p2[q];
-            }
-        }
-    }
-    *s0 = a0;
-    *s1 = a1;
-    *s2 = a2;
+__device__ __forceinline__ TileGeo inst_tile(const ImpInst& I, int vt, int c, int lane) {
+    return tile_geo(I.nt_neg, I.kp, I.nv, I.n_inner, I.rows, vt, c, lane);
 }
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// ---- tile geometry --------------------------------------------------------
-struct TileGeo {
-    bool pos;      // velocities > 0 -> forward scan
-    int j;         // this lane's velocity index
-    bool lane_ok;
-    int s0;        // first scan position of the tile
-};
-
-__device__ __forceinline__ TileGeo tile_geo(const ImpInst& I, int vt, int c, int lane) {
-    TileGeo g;
-    g.pos = vt >= I.nt_neg;
-    g.j = g.pos ? I.kp + 32 * (vt - I.nt_neg) + lane : I.kp - 32 * (vt + 1) + lane;
-    g.lane_ok = g.pos ? (g.j < I.nv) : (g.j >= 0);
-    g.s0 = c * kR;
-    return g;
-}
-
-__device__ __forceinline__ int scan_row(int nx, bool pos, int s) { return pos ? 1 + s : nx - 2 - s; }
 
 // Copy an instance descriptor into the warp's shared memory.  Reads of the
 // descriptor then cannot alias the warp's global stores.
@@ -255,64 +186,84 @@ __device__ __forceinline__ void stage_warp(WarpSmem& w, const ImpInst* src, int 
         int* d = reinterpret_cast<int*>(&w.I);
         for (int q = lane; q < (int)(sizeof(ImpInst) / sizeof(int)); q += 32) d[q] = __ldg(s + q);
         __syncwarp();
-        if (lane == 0) w.cur_b = b;
+        if (lane == 0) {
+            w.cur_b = b;
+            w.cur_m = -1;
+        }
     }
     __syncwarp();
 }
 
-// Reduce-scatter of the 3 moments of 8 rows held per lane and store of the
-// per-(v-tile,row) partials; rows s0 + 8*q8 .. +7.
-__device__ __forceinline__ void store_partials8(const ImpInst& I, const TileGeo& g, int vt, int lane,
-                                                double (&acc)[24], int q8) {
-    warp_reduce_scatter<8, 3>(acc, lane);
-    if (owner_writes<8>(lane)) {
-        const int s = g.s0 + 8 * q8 + owner_row<8>(lane);
-        if (s < I.n_inner) {
-            const int k = scan_row(I.nx, g.pos, s) - 1;
-            double* p = I.part + ((size_t)vt * I.n_inner + k) * kPartQ;
-            p[0] = acc[0];
-            p[1] = acc[1];
-            p[2] = acc[2];
+// Activity of the staged instance in iteration m, cached per warp.
+__device__ __forceinline__ bool staged_active(WarpSmem& w, int m) {
+    if (w.cur_m != m) {
+        const bool a = inst_active(w.I, m);
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) {
+            w.cur_active = a ? 1 : 0;
+            w.cur_m = m;
         }
+        __syncwarp();
     }
+    return w.cur_active != 0;
 }
 
-// ---- P1: partial moments of f^n (one warp-tile) -------------------------
-__device__ void moments_wtile(const ImpInst& I, int vt, int c, const double* __restrict__ f) {
+// Asynchronous copy of a tile's rows into shared memory (one 8-byte element
+// per lane and row, all rows in flight at once).
+template <int STRIDE>
+__device__ __forceinline__ void stage_rows(double (*dst)[STRIDE], const double* __restrict__ src,
+                                           const TileGeo& g, int nx, int nv) {
     const int lane = threadIdx.x & 31;
-    const TileGeo g = tile_geo(I, vt, c, lane);
-    const double vj = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
-#pragma unroll 1
-    for (int q8 = 0; q8 < kR / 8; ++q8) {
-        double acc[24];
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            const int s = g.s0 + 8 * q8 + r;
-            double x = 0.0;
-            if (s < I.n_inner && g.lane_ok) x = f[(size_t)scan_row(I.nx, g.pos, s) * I.nv + g.j];
-            acc[3 * r + 0] = x;
-            acc[3 * r + 1] = x * vj;
-            acc[3 * r + 2] = x * vj * vj;
-        }
-        store_partials8(I, g, vt, lane, acc, q8);
-    }
+    if (!g.lane_ok) return;
+#pragma unroll 8
+    for (int r = 0; r < g.nrows; ++r)
+        cp_async8(&dst[r][lane], src + (size_t)scan_row(nx, g.pos, g.s0 + r) * nv + g.j);
 }
 
-// Row coefficients of W^(m) for the warp-tile's rows into w.coef (lane r
-// handles row r).  After an applied Anderson call the combination
+// Store the per-(v-tile, row) partial moments of the tile held in w.a
+// (lane r sums row r over the 32 columns).
+__device__ __forceinline__ void store_partials(WarpSmem& w, const TileGeo& g, int vt) {
+    const ImpInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    if (lane < g.nrows) {
+        double s[4];
+        row_sums4(w.a, w.vv, lane, s);
+        const int k = scan_row(I.nx, g.pos, g.s0 + lane) - 1;
+        double* p = I.part + ((size_t)vt * I.n_inner + k) * kPartQ;
+        reinterpret_cast<double2*>(p)[0] = make_double2(s[0], s[1]);
+        reinterpret_cast<double2*>(p)[1] = make_double2(s[2], s[3]);
+    }
+    __syncwarp();
+}
+
+// ---- P1: partial moments of f^n (one tile) -------------------------------
+__device__ void moments_tile(WarpSmem& w, int vt, int c, const double* __restrict__ f) {
+    const ImpInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const TileGeo g = inst_tile(I, vt, c, lane);
+    stage_rows<33>(w.a, f, g, I.nx, I.nv);
+    cp_async_commit();
+    w.vv[lane] = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
+    cp_async_wait_all();
+    if (!g.lane_ok)
+        for (int r = 0; r < g.nrows; ++r) w.a[r][lane] = 0.0;
+    store_partials(w, g, vt);
+}
+
+// Row coefficients of W^(m) for the tile's rows into w.coef (lane r handles
+// row r).  After an applied Anderson call the combination
 // w = beta G alpha + (1-beta) w_new with floors and |u| <= u_max
 // (bgk1d_aa_cpu.py:170-188) is formed from the history ring; tiles of v-tile 0
-// then publish W^(m) and its coefficients for pass 2 and the reduction.
-__device__ __forceinline__ void stage_coeffs(WarpSmem& w, const TileGeo& g, int vt, int m,
-                                             bool pass1) {
+// then publish W^(m) and its coefficients for the reduction.
+__device__ __forceinline__ void stage_coeffs(WarpSmem& w, const TileGeo& g, int vt, int m) {
     const ImpInst& I = w.I;
     const int lane = threadIdx.x & 31;
     const int nx = I.nx, n_inner = I.n_inner;
-    const int s = g.s0 + lane;
     double c4[4] = {0.0, 0.0, 0.0, 0.0};
-    if (s < n_inner) {
-        const int i = scan_row(nx, g.pos, s);
-        if (pass1 && m >= 1 && aa_applies(I, m - 1)) {
+    if (lane < g.nrows) {
+        const int i = scan_row(nx, g.pos, g.s0 + lane);
+        if (m >= 1 && aa_applies(I, m - 1)) {
             const int k = i - 1, d = 3 * n_inner;
             const int mh = m < I.aa_cols ? m : I.aa_cols;
             const int head_out = m % I.aa_cols;
@@ -361,241 +312,86 @@ __device__ __forceinline__ void stage_coeffs(WarpSmem& w, const TileGeo& g, int 
     for (int q = 0; q < 4; ++q) w.coef[lane][q] = c4[q];
 }
 
-// ---- pass 1: the affine map x_out = P x_in + Y of one warp-tile ------------
-// For v > 0 the upwind implicit row is x_i = (b_i + alpha x_{i-1}) / d_i with
-// d_i = 1 + alpha + dt/tau_i and b_i = f^n_i + dt/tau_i M_i(v)
-// (implicit_kernels.cu:104-131); v <= 0 is the mirror image in x.  Written as
-// x_s = a_s x_{s-1} + c_s with a_s = alpha/d_s, c_s = b_s/d_s.  Pass 1 stores
-// c (the only part that needs the Maxwellian) and the tile map; the last tile
-// of each group of kGroup chunks of a velocity column also stores the
-// group's composed map.
-constexpr int kGroup = 8;
-
-__device__ __forceinline__ void load_rows8(double (&v)[8], const double* __restrict__ src,
-                                           const TileGeo& g, int q8, int nx, int nv,
-                                           int n_inner) {
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-        const int s = g.s0 + 8 * q8 + t;
-        v[t] = (s < n_inner && g.lane_ok) ? src[(size_t)scan_row(nx, g.pos, s) * nv + g.j] : 0.0;
-    }
-}
-
-// Asynchronous copy of a warp-tile (kR rows x 32 velocities) into shared
-// memory, one 8-byte element per lane and row (all rows in flight at once).
-__device__ __forceinline__ void stage_tile(double (&dst)[kR][32], const double* __restrict__ src,
-                                           const TileGeo& g, int nx, int nv, int n_inner) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll 8
-    for (int r = 0; r < kR; ++r) {
-        const int s = g.s0 + r;
-        if (s < n_inner && g.lane_ok)
-            cp_async8(&dst[r][lane], src + (size_t)scan_row(nx, g.pos, s) * nv + g.j);
-    }
-}
-
-__device__ void map_wtile(WarpSmem& w, int vt, int c, int m, const double* __restrict__ fn) {
+// ---- the Picard pass over one tile ------------------------------------------
+// Assembly of the tile's rows (x_s = a_s x_{s-1} + c_s with a_s = alpha/d_s,
+// c_s = b_s/d_s), look-back for the carry, recurrence, residual against
+// f^(m) and partial moments of f^(m+1).  Returns false if the look-back gave
+// up (timeout).
+__device__ bool picard_tile(WarpSmem& w, int vt, int c, int m, unsigned long long epoch,
+                            unsigned long long limit, const double* __restrict__ fn,
+                            double* __restrict__ fo, FracMax& q1, FracMax& q2, bool& bad) {
     const ImpInst& I = w.I;
     const int lane = threadIdx.x & 31;
-    const TileGeo g = tile_geo(I, vt, c, lane);
-    const int nx = I.nx, nv = I.nv, n_inner = I.n_inner, nvt = I.nvt;
-    stage_tile(w.buf0, fn, g, nx, nv, n_inner);
+    const TileGeo g = inst_tile(I, vt, c, lane);
+    const int nx = I.nx, nv = I.nv;
+    const int nr = g.nrows;
+    // f^n rows and the residual reference f^(m) (f^n itself at m = 0)
+    stage_rows<33>(w.a, fn, g, nx, nv);
+    stage_rows<32>(w.o, m > 0 ? fo : fn, g, nx, nv);
     cp_async_commit();
     const double vj = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
-    stage_coeffs(w, g, vt, m, true);
+    w.vv[lane] = vj;
+    stage_coeffs(w, g, vt, m);
     cp_async_wait_all();
     __syncwarp();
     const double cpl = I.dtdx * fabs(vj);  // alpha (v>0) or beta (v<0)
     const double one_plus = 1.0 + cpl;     // 1 + alpha + beta
+    // tile map: c_s into w.a, (P, Y) composed in scan order
     double P = 1.0, Y = 0.0;
 #pragma unroll 1
-    for (int q8 = 0; q8 < kR / 8; ++q8) {
+    for (int r0 = 0; r0 < nr; r0 += 8) {
         double av[8], cv[8];
 #pragma unroll
         for (int t = 0; t < 8; ++t) {
-            const int r = 8 * q8 + t;
+            const int r = r0 + t < nr ? r0 + t : nr - 1;
             const double diff = vj - w.coef[r][0];
             const double dti = w.coef[r][3];
             const double M = w.coef[r][2] * exp_nonpos(diff * diff * w.coef[r][1]);
             const double rr = recip_ge1(one_plus + dti);
-            cv[t] = fma(dti, M, w.buf0[r][lane]) * rr;
+            const double fnv = g.lane_ok ? w.a[r][lane] : 0.0;
+            cv[t] = fma(dti, M, fnv) * rr;
             av[t] = cpl * rr;
         }
 #pragma unroll
         for (int t = 0; t < 8; ++t) {
-            const int s = g.s0 + 8 * q8 + t;
-            if (s < n_inner && g.lane_ok) {
-                I.crhs[(size_t)scan_row(nx, g.pos, s) * nv + g.j] = cv[t];
+            if (r0 + t < nr) {
+                w.a[r0 + t][lane] = cv[t];
                 Y = fma(av[t], Y, cv[t]);
                 P = P * av[t];
             }
         }
     }
-    const size_t tid = (size_t)c * nvt + vt;
-    I.agg[tid * 64 + lane] = P;
-    I.agg[tid * 64 + 32 + lane] = Y;
-
-    // last tile of this group of chunks composes the group map (nested, in x order)
-    const int grp = c / kGroup, ngroups = (I.nchunks + kGroup - 1) / kGroup;
-    fence_acq_rel();
-    __syncwarp();
-    unsigned prev = 0;
-    if (lane == 0) prev = atomicAdd(&I.grpcnt[((size_t)m * nvt + vt) * ngroups + grp], 1u);
-    prev = __shfl_sync(0xffffffffu, prev, 0);
-    const int c0 = grp * kGroup, c1 = (c0 + kGroup < I.nchunks ? c0 + kGroup : I.nchunks);
-    if (prev == (unsigned)(c1 - c0) - 1) {
-        fence_acq_rel();
-        __syncwarp();
-        double Pk[kGroup], Yk[kGroup];
-#pragma unroll
-        for (int q = 0; q < kGroup; ++q) {
-            Pk[q] = 1.0;
-            Yk[q] = 0.0;
-            if (c0 + q < c1) {
-                const double* a = I.agg + ((size_t)(c0 + q) * nvt + vt) * 64;
-                Pk[q] = ld_cg(a + lane);
-                Yk[q] = ld_cg(a + 32 + lane);
-            }
-        }
-        double GP = 1.0, GY = 0.0;
-#pragma unroll
-        for (int q = 0; q < kGroup; ++q) {
-            if (c0 + q < c1) {
-                GY = fma(Pk[q], GY, Yk[q]);
-                GP = Pk[q] * GP;
-            }
-        }
-        double* gm = I.gmap + ((size_t)vt * ngroups + grp) * 64;
-        gm[lane] = GP;
-        gm[32 + lane] = GY;
+    // carry into the tile
+    const size_t tid = (size_t)c * I.nvt + vt;
+    bool ok = true;
+    double X;
+    if (c == 0) {
+        X = g.lane_ok ? __ldg(&fn[(size_t)(g.pos ? 0 : nx - 1) * nv + g.j]) : 0.0;
+    } else {
+        publish_agg(I.agg, I.flag, tid, P, Y, epoch);
+        ok = lookback(I.agg, I.inc, I.flag, I.nvt, vt, c, epoch, limit, X);
     }
-    __syncwarp();
-}
-
-// Carry into chunk c of column vt: the boundary value pushed through the
-// group maps of the groups before c's group, then through the chunk maps of
-// c's group before c -- a fixed nested order, so every tile (and every run)
-// gets the same value.
-__device__ __forceinline__ double tile_carry(const ImpInst& I, const TileGeo& g, int vt, int c,
-                                             const double* __restrict__ fn) {
-    const int lane = threadIdx.x & 31;
-    const int nvt = I.nvt, ngroups = (I.nchunks + kGroup - 1) / kGroup;
-    const int grp = c / kGroup;
-    double X = g.lane_ok ? fn[(size_t)(g.pos ? 0 : I.nx - 1) * I.nv + g.j] : 0.0;
-    for (int g0 = 0; g0 < grp; g0 += 8) {
-        double Pq[8], Yq[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            Pq[q] = 1.0;
-            Yq[q] = 0.0;
-            if (g0 + q < grp) {
-                const double* gm = I.gmap + ((size_t)vt * ngroups + g0 + q) * 64;
-                Pq[q] = ld_cg(gm + lane);
-                Yq[q] = ld_cg(gm + 32 + lane);
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q)
-            if (g0 + q < grp) X = fma(Pq[q], X, Yq[q]);
-    }
-    const int c0 = grp * kGroup;
-    double Pk[kGroup], Yk[kGroup];
-#pragma unroll
-    for (int q = 0; q < kGroup; ++q) {
-        Pk[q] = 1.0;
-        Yk[q] = 0.0;
-        if (c0 + q < c) {
-            const double* a = I.agg + ((size_t)(c0 + q) * nvt + vt) * 64;
-            Pk[q] = ld_cg(a + lane);
-            Yk[q] = ld_cg(a + 32 + lane);
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < kGroup; ++q)
-        if (c0 + q < c) X = fma(Pk[q], X, Yk[q]);
-    return X;
-}
-
-// ---- pass 2: solve of one warp-tile from its carry; residual, moments -----
-// Re-forms a_s (no exponential) and reads c_s; returns (in w.done_rb) the
-// row blocks this tile completed.
-__device__ void solve_wtile(WarpSmem& w, int vt, int c, int m, const double* __restrict__ fn,
-                            double* __restrict__ fo, FracMax& q1, FracMax& q2, bool& bad) {
-    const ImpInst& I = w.I;
-    const int lane = threadIdx.x & 31;
-    const TileGeo g = tile_geo(I, vt, c, lane);
-    const int nx = I.nx, nv = I.nv, n_inner = I.n_inner;
-    // residual reference: f^(m) (this kernel's previous iterate), or f^n at m = 0
-    const double* fref = m > 0 ? fo : fn;
-    stage_tile(w.buf0, I.crhs, g, nx, nv, n_inner);
-    stage_tile(w.buf1, fref, g, nx, nv, n_inner);
-    cp_async_commit();
-    const double vj = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
-    stage_coeffs(w, g, vt, m, false);
-    double X = tile_carry(I, g, vt, c, fn);
-    cp_async_wait_all();
-    __syncwarp();
-    const double cpl = I.dtdx * fabs(vj);
-    const double one_plus = 1.0 + cpl;
+    if (c + 1 < I.nchunks) publish_inc(I.inc, I.flag, tid, fma(P, X, Y), epoch);
+    // recurrence, write, residual
     const double tol = I.tol, abs_tol = I.abs_tol;
-#pragma unroll 1
-    for (int q4 = 0; q4 < kR / 4; ++q4) {
-        double acc[12];
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-            const int s = g.s0 + 4 * q4 + t;
-            double x = 0.0;
-            if (s < n_inner && g.lane_ok) {
-                const double a = cpl * recip_ge1(one_plus + w.coef[4 * q4 + t][3]);
-                X = fma(a, X, w.buf0[4 * q4 + t][lane]);
-                x = X;
-                fo[(size_t)scan_row(nx, g.pos, s) * nv + g.j] = x;
-                const double o = w.buf1[4 * q4 + t][lane];
-                const double df = fabs(x - o);
-                const double ref = nan_max(fabs(x), fabs(o));
-                q1.add(df, abs_tol + tol * ref);
-                q2.add(df, (ref != ref || ref >= abs_tol) ? ref : abs_tol);
-                bad |= !isfinite(x);
-            }
-            acc[3 * t + 0] = x;
-            acc[3 * t + 1] = x * vj;
-            acc[3 * t + 2] = x * vj * vj;
-        }
-        warp_reduce_scatter<4, 3>(acc, lane);
-        if (owner_writes<4>(lane)) {
-            const int s = g.s0 + 4 * q4 + owner_row<4>(lane);
-            if (s < n_inner) {
-                const int k = scan_row(nx, g.pos, s) - 1;
-                double* p = I.part + ((size_t)vt * n_inner + k) * kPartQ;
-                p[0] = acc[0];
-                p[1] = acc[1];
-                p[2] = acc[2];
-            }
+#pragma unroll 4
+    for (int r = 0; r < nr; ++r) {
+        const double a = cpl * recip_ge1(one_plus + w.coef[r][3]);
+        X = fma(a, X, w.a[r][lane]);
+        const double x = g.lane_ok ? X : 0.0;
+        w.a[r][lane] = x;
+        if (g.lane_ok) {
+            fo[(size_t)scan_row(nx, g.pos, g.s0 + r) * nv + g.j] = x;
+            const double o = w.o[r][lane];
+            const double df = fabs(x - o);
+            const double ref = nan_max(fabs(x), fabs(o));
+            q1.add(df, abs_tol + tol * ref);
+            q2.add(df, (ref != ref || ref >= abs_tol) ? ref : abs_tol);
+            bad |= !isfinite(x);
         }
     }
-
-    // row-block arrival counting (rows x v-tiles); a block whose count
-    // completes is reduced by this warp right away
-    fence_acq_rel();
-    __syncwarp();
-    if (lane == 0) {
-        w.done_rb[0] = -1;
-        w.done_rb[1] = -1;
-        const int s_lo = g.s0, s_hi = (g.s0 + kR < n_inner ? g.s0 + kR : n_inner) - 1;
-        const int k_a = scan_row(nx, g.pos, s_lo) - 1, k_b = scan_row(nx, g.pos, s_hi) - 1;
-        const int k_lo = k_a < k_b ? k_a : k_b, k_hi = k_a < k_b ? k_b : k_a;
-        int nd = 0;
-        for (int rb = k_lo / kR; rb <= k_hi / kR; ++rb) {
-            const int lo = rb * kR > k_lo ? rb * kR : k_lo;
-            const int hi = (rb + 1) * kR - 1 < k_hi ? (rb + 1) * kR - 1 : k_hi;
-            const unsigned add = (unsigned)(hi - lo + 1);
-            const int rows_in_rb = ((rb + 1) * kR < n_inner ? (rb + 1) * kR : n_inner) - rb * kR;
-            const unsigned expect = (unsigned)rows_in_rb * (unsigned)I.nvt;
-            const unsigned prev = atomicAdd(&I.rbcnt[(size_t)m * I.nrb + rb], add);
-            if (prev + add == expect) w.done_rb[nd++] = rb;
-        }
-    }
-    __syncwarp();
+    store_partials(w, g, vt);
+    return ok;
 }
 
 // ---- Anderson: small symmetric solve (Cholesky, min-norm fall-back) -------
@@ -717,15 +513,15 @@ __device__ __noinline__ void aa_finalize(const double* gpart, int nrb, int mh, d
 __device__ __noinline__ void reduce_block(WarpSmem& w, int ru, int m) {
     const ImpInst& I = w.I;
     const int lane = threadIdx.x & 31;
-    const int k = ru * kR + lane;
+    const int k = ru * kRB + lane;
     const bool ok = k < I.n_inner;
     const int i = k + 1;
     const int nx = I.nx, n_inner = I.n_inner, d = 3 * n_inner;
     double wn[3] = {0.0, 0.0, 0.0}, wo[3] = {0.0, 0.0, 0.0};
     if (ok) {
-        double s0, s1, s2;
-        sum_partials(I.part, I.nvt, n_inner, k, &s0, &s1, &s2);
-        moments_from_sums(s0, s1, s2, I.dv, &wn[0], &wn[1], &wn[2]);
+        double s[4];
+        sum_partials4(I.part, 0, I.nvt, n_inner, k, s);
+        moments_from_sums(s[0], s[1], s[2], I.dv, &wn[0], &wn[1], &wn[2]);
         wo[0] = ld_cg(&I.W[i]);
         wo[1] = ld_cg(&I.W[nx + i]);
         wo[2] = ld_cg(&I.W[2 * nx + i]);
@@ -842,13 +638,13 @@ __device__ __noinline__ void reduce_block(WarpSmem& w, int ru, int m) {
 __device__ void init_block(WarpSmem& w, int ru) {
     const ImpInst& I = w.I;
     const int lane = threadIdx.x & 31;
-    const int k = ru * kR + lane;
+    const int k = ru * kRB + lane;
     const int nx = I.nx, n_inner = I.n_inner;
     if (k < n_inner) {
-        double s0, s1, s2;
-        sum_partials(I.part, I.nvt, n_inner, k, &s0, &s1, &s2);
+        double s[4];
+        sum_partials4(I.part, 0, I.nvt, n_inner, k, s);
         double n, nu, T;
-        moments_from_sums(s0, s1, s2, I.dv, &n, &nu, &T);
+        moments_from_sums(s[0], s[1], s[2], I.dv, &n, &nu, &T);
         const int i = k + 1;
         I.W[i] = n;
         I.W[nx + i] = nu;
@@ -880,9 +676,8 @@ __device__ __forceinline__ void flush_residual(const ImpInst& I, int m, FracMax&
 }
 
 // Phase trace (off unless a buffer is attached): per Picard iteration the
-// earliest start and latest end over all warps of pass 1 and pass 2, in
-// %globaltimer nanoseconds: [m][0] min start p1, [1] max end p1, [2] min start
-// p2, [3] max end p2; row kTraceRows-1 holds the prologue.
+// earliest start and latest end over all warps of the pass, in
+// %globaltimer nanoseconds: [m][0] min start, [1] max end; [2], [3] unused.
 constexpr int kTracePhases = 4;
 __device__ __forceinline__ unsigned long long gtimer() {
     unsigned long long t;
@@ -890,8 +685,8 @@ __device__ __forceinline__ unsigned long long gtimer() {
     return t;
 }
 __device__ __forceinline__ void trace_mark(const PlanDev& P, int m, int ph, bool is_min) {
-    if (P.trace == nullptr || (threadIdx.x & 31) != 0 || m >= P.trace_iters) return;
-    unsigned long long* slot = P.trace + (size_t)m * kTracePhases + ph;
+    if (P.head.trace == nullptr || (threadIdx.x & 31) != 0 || m >= P.head.trace_iters) return;
+    unsigned long long* slot = P.head.trace + (size_t)m * kTracePhases + ph;
     const unsigned long long t = gtimer();
     if (is_min) atomicMin(slot, t); else atomicMax(slot, t);
 }
@@ -899,17 +694,23 @@ __device__ __forceinline__ void trace_mark(const PlanDev& P, int m, int ph, bool
 // Grid barrier of a launch; on a timeout the error is also recorded in the
 // sticky word read by keq_plan_error.
 __device__ __forceinline__ bool plan_sync(PlanDev& P, unsigned G) {
-    if (grid_sync(&P.bar, G, &P.err, P.spin_limit)) return true;
-    if (threadIdx.x == 0) atomicOr(&P.err_sticky, 1 << KEQ_ERR_TIMEOUT);
+    if (grid_sync(&P.head.bar, G, &P.head.err, P.head.spin_limit)) return true;
+    if (threadIdx.x == 0) atomicOr(&P.head.err_sticky, 1 << KEQ_ERR_TIMEOUT);
     return false;
 }
 
+// Next tile ticket of iteration m (lane 0 claims, broadcast to the warp).
+__device__ __forceinline__ long long claim(unsigned* tickets, int m) {
+    unsigned t = 0;
+    if ((threadIdx.x & 31) == 0) t = atomicAdd(&tickets[m], 1u);
+    return (long long)__shfl_sync(0xffffffffu, t, 0);
+}
+
 // ---- the persistent kernel --------------------------------------------------
-// Work items (warp-tiles, row blocks) are statically strided over all
-// resident warps of the cooperative grid.  Inside a phase no warp waits for
-// another: pass 1 and pass 2 are separated by a grid barrier, and the column
-// scans and row reductions are done by whichever warp completes a column or a
-// row block (arrival counters).
+// P1 tiles and row blocks are statically strided over all resident warps.
+// The Picard pass claims tiles from a ticket counter so tiles are started in
+// x order (chunk-major), which keeps every look-back short and guarantees
+// that a tile's predecessors are held by running warps.
 __global__ void __launch_bounds__(kThreads, 3)
 implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -924,6 +725,10 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
     __syncwarp();
 
     // P0: reset per-step state, boundary rows of f_out, boundary-row moments
+    if (blockIdx.x == 0) {
+        for (int q = threadIdx.x; q < P.max_iter; q += kThreads) P.tickets[q] = 0u;
+        if (threadIdx.x == 0) P.head.seq = P.head.seq + 1ull;
+    }
     for (int b = blockIdx.x; b < n_inst; b += G) {
         const ImpInst& I = P.inst[b];
         const double* fn = swap_io ? I.f_out : I.f_in;
@@ -937,9 +742,6 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
             I.nonfin[q] = 0;
             I.rbdone[q] = 0u;
         }
-        for (int q = threadIdx.x; q < I.picard_iter * I.nvt * ((I.nchunks + kGroup - 1) / kGroup);
-             q += kThreads)
-            I.grpcnt[q] = 0u;
         for (int q = threadIdx.x; q < I.picard_iter * I.nrb; q += kThreads) I.rbcnt[q] = 0u;
         for (int q = threadIdx.x; q < I.nv; q += kThreads) {
             fo[q] = fn[q];
@@ -963,6 +765,8 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
         }
     }
     if (!plan_sync(P, G)) return;
+    const unsigned long long seq = __ldcg(&P.head.seq);
+    const unsigned long long limit = P.head.spin_limit;
 
     // P1: moments of f^n
     for (long long t = gwarp; t < total_tiles; t += nwarps) {
@@ -970,7 +774,7 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
         stage_warp(w, &P.inst[b], b);
         const long long tl = t - w.I.tile_off;
         const int c = (int)(tl / w.I.nvt), vt = (int)(tl % w.I.nvt);
-        moments_wtile(w.I, vt, c, swap_io ? w.I.f_out : w.I.f_in);
+        moments_tile(w, vt, c, swap_io ? w.I.f_out : w.I.f_in);
     }
     if (!plan_sync(P, G)) return;
 
@@ -987,37 +791,38 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
         bool any = false;
         for (int b = 0; b < n_inst && !any; ++b) any = inst_active(P.inst[b], m);
         if (!any) break;
+        const unsigned long long epoch = seq * (unsigned long long)(P.max_iter + 1) + m + 1;
 
-        // pass 1: tile maps and group maps
         trace_mark(P, m, 0, true);
-        for (long long t = gwarp; t < total_tiles; t += nwarps) {
-            const int b = find_inst(P.tile_off, n_inst, t);
-            stage_warp(w, &P.inst[b], b);
-            if (!inst_active(w.I, m)) continue;
-            const long long tl = t - w.I.tile_off;
-            const int c = (int)(tl / w.I.nvt), vt = (int)(tl % w.I.nvt);
-            map_wtile(w, vt, c, m, swap_io ? w.I.f_out : w.I.f_in);
-        }
-        trace_mark(P, m, 1, false);
-        if (!plan_sync(P, G)) return;
-        trace_mark(P, m, 2, true);
-
-        // pass 2: solve, residual, partial moments; completed row blocks are
-        // reduced on the spot (W update, Anderson history and Gram matrix)
         FracMax q1, q2;
         bool bad = false;
         int res_b = -1;
-        for (long long t = gwarp; t < total_tiles; t += nwarps) {
+        for (;;) {
+            const long long t = claim(P.tickets, m);
+            if (t >= total_tiles) break;
             const int b = find_inst(P.tile_off, n_inst, t);
-            if (b != res_b && res_b >= 0) flush_residual(w.I, m, q1, q2, bad);
+            if (b != res_b && res_b >= 0 && staged_active(w, m)) flush_residual(w.I, m, q1, q2, bad);
             stage_warp(w, &P.inst[b], b);
             res_b = b;
-            if (!inst_active(w.I, m)) continue;
+            if (!staged_active(w, m)) continue;
             const long long tl = t - w.I.tile_off;
             const int c = (int)(tl / w.I.nvt), vt = (int)(tl % w.I.nvt);
             const double* fn = swap_io ? w.I.f_out : w.I.f_in;
             double* fo = swap_io ? const_cast<double*>(w.I.f_in) : w.I.f_out;
-            solve_wtile(w, vt, c, m, fn, fo, q1, q2, bad);
+            if (!picard_tile(w, vt, c, m, epoch, limit, fn, fo, q1, q2, bad)) {
+                if (lane == 0) {
+                    atomicOr(&P.head.err, 1 << KEQ_ERR_TIMEOUT);
+                    atomicOr(&P.head.err_sticky, 1 << KEQ_ERR_TIMEOUT);
+                }
+            }
+            // row-block arrivals; a completed block is reduced right away
+            const TileGeo g = inst_tile(w.I, vt, c, lane);
+            fence_acq_rel();
+            __syncwarp();
+            if (lane == 0)
+                rowblock_arrive(w.I.rbcnt + (size_t)m * w.I.nrb, w.I.nx, w.I.n_inner, w.I.nvt, g,
+                                w.done_rb);
+            __syncwarp();
             const int d0 = w.done_rb[0], d1 = w.done_rb[1];
             if (d0 >= 0 || d1 >= 0) {
                 fence_acq_rel();
@@ -1026,8 +831,8 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
                 if (d1 >= 0) reduce_block(w, d1, m);
             }
         }
-        if (res_b >= 0 && inst_active(w.I, m)) flush_residual(w.I, m, q1, q2, bad);
-        trace_mark(P, m, 3, false);
+        if (res_b >= 0 && staged_active(w, m)) flush_residual(w.I, m, q1, q2, bad);
+        trace_mark(P, m, 1, false);
         if (!plan_sync(P, G)) return;
     }
 
@@ -1046,7 +851,7 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
             if (aa_applies(I, m)) ++aa_applied;
         int status = KEQ_OK;
         if (last >= 0 && __ldcg(&I.nonfin[last])) status = KEQ_ERR_NONFINITE;
-        if (__ldcg(&P.err) & (1 << KEQ_ERR_TIMEOUT)) status = KEQ_ERR_TIMEOUT;
+        if (__ldcg(&P.head.err) & (1 << KEQ_ERR_TIMEOUT)) status = KEQ_ERR_TIMEOUT;
         s->status = status;
         s->iters = last + 1;
         s->aa_applied = aa_applied;
@@ -1088,8 +893,13 @@ struct Carve {
 };
 
 struct Derived {
-    int n_inner, nt_neg, nt_pos, nvt, nchunks, nrb, aa_cols, aa_on;
+    int n_inner, nt_neg, nt_pos, nvt, rows, nchunks, nrb, aa_cols, aa_on;
 };
+
+int tile_rows_of(const keq_implicit_params& p) {
+    const int r = p.tile_rows;
+    return (r == 8 || r == 16 || r == 24 || r == 32) ? r : keq::kRmax;
+}
 
 Derived derive(int nx, int nv, int kp, const keq_implicit_params& p) {
     Derived d;
@@ -1097,8 +907,9 @@ Derived derive(int nx, int nv, int kp, const keq_implicit_params& p) {
     d.nt_neg = (kp + 31) / 32;
     d.nt_pos = (nv - kp + 31) / 32;
     d.nvt = d.nt_neg + d.nt_pos;
-    d.nchunks = (d.n_inner + keq::kR - 1) / keq::kR;
-    d.nrb = (d.n_inner + keq::kR - 1) / keq::kR;
+    d.rows = tile_rows_of(p);
+    d.nchunks = (d.n_inner + d.rows - 1) / d.rows;
+    d.nrb = (d.n_inner + keq::kRB - 1) / keq::kRB;
     const int aa_m = p.aa_m > 0 ? p.aa_m : 0;
     d.aa_on = (p.aa_enable && aa_m >= 1 && aa_m + 1 >= 2) ? 1 : 0;
     d.aa_cols = d.aa_on ? aa_m + 1 : 1;
@@ -1112,16 +923,15 @@ size_t carve_instance(void* base, int nx, int nv, int kp, const keq_implicit_par
     const Derived d = derive(nx, nv, kp, p);
     Carve c{static_cast<char*>(base), 0};
     const int it = p.picard_iter > 0 ? p.picard_iter : 1;
+    const size_t ntiles = (size_t)d.nvt * d.nchunks;
     double* W = c.take<double>(3 * (size_t)nx);
     double* Wn = c.take<double>(3 * (size_t)nx);
     double* Wc = c.take<double>(4 * (size_t)nx);
     double* Wb = c.take<double>(8);
     double* part = c.take<double>((size_t)d.nvt * d.n_inner * keq::kPartQ);
-    const int ngroups = (d.nchunks + keq::kGroup - 1) / keq::kGroup;
-    double* agg = c.take<double>((size_t)d.nvt * d.nchunks * 64);
-    double* gmap = c.take<double>((size_t)d.nvt * ngroups * 64);
-    double* crhs = c.take<double>((size_t)nx * nv);
-    unsigned* grpcnt = c.take<unsigned>((size_t)it * d.nvt * ngroups);
+    double* agg = c.take<double>(ntiles * 64);
+    double* inc = c.take<double>(ntiles * 32);
+    unsigned long long* flag = c.take<unsigned long long>(ntiles);
     unsigned* rbcnt = c.take<unsigned>((size_t)it * d.nrb);
     double* res = c.take<double>(2 * (size_t)it);
     int* st = c.take<int>(it);
@@ -1133,20 +943,20 @@ size_t carve_instance(void* base, int nx, int nv, int kp, const keq_implicit_par
     unsigned* rbdone = c.take<unsigned>(it);
     if (I) {
         I->W = W; I->Wn = Wn; I->Wc = Wc; I->Wb = Wb; I->part = part; I->agg = agg;
-        I->gmap = gmap; I->crhs = crhs; I->grpcnt = grpcnt; I->rbcnt = rbcnt; I->res = res; I->st = st; I->nonfin = nonfin; I->aaG = aaG;
-        I->aaR = aaR; I->gpart = gpart; I->alpha = alpha; I->rbdone = rbdone;
+        I->inc = inc; I->flag = flag; I->rbcnt = rbcnt; I->res = res; I->st = st;
+        I->nonfin = nonfin; I->aaG = aaG; I->aaR = aaR; I->gpart = gpart; I->alpha = alpha;
+        I->rbdone = rbdone;
     }
     return align_up(c.off, 256);
 }
-
-// Worst-case kp for sizing before v is known on the host: the tile count is
-// maximal when the sign change is not 32-aligned.
-int sizing_kp(int nv) { return nv / 2 + 1 <= nv ? nv / 2 + 1 : nv; }
 
 bool valid_params(const keq_implicit_params& p) {
     if (p.picard_iter < 1 || p.picard_iter > 100000) return false;
     if (p.conv_type != 0 && p.conv_type != 1) return false;
     if (p.aa_enable && p.aa_m > keq::kMaxAACols - 1) return false;
+    if (p.tile_rows != 0 && p.tile_rows != 8 && p.tile_rows != 16 && p.tile_rows != 24 &&
+        p.tile_rows != 32)
+        return false;
     return true;
 }
 
@@ -1164,16 +974,6 @@ keq_implicit_params normalized(const keq_implicit_params& in) {
 
 }  // namespace
 
-struct keq_plan {
-    std::vector<ImpInst> host_inst;
-    std::vector<long long> tile_off, rb_off;
-    PlanDev* dev;           // device header (inside the plan workspace)
-    ImpInst* dev_inst;
-    int grid;
-    int n_inst;
-    int device;
-};
-
 extern "C" {
 
 keq_status keq_implicit_instance_workspace_size(const keq_grid* grid,
@@ -1183,15 +983,17 @@ keq_status keq_implicit_instance_workspace_size(const keq_grid* grid,
     if (grid->nx < 3 || grid->nv < 1) return KEQ_ERR_INVALID;
     if (!valid_params(*params)) return KEQ_ERR_INVALID;
     const keq_implicit_params p = normalized(*params);
-    *bytes = carve_instance(nullptr, grid->nx, grid->nv, sizing_kp(grid->nv), p, nullptr);
-    // the tile count is maximal for some kp; take the max over both extremes
-    const size_t b2 = carve_instance(nullptr, grid->nx, grid->nv, 0, p, nullptr);
-    const size_t b3 = carve_instance(nullptr, grid->nx, grid->nv, grid->nv, p, nullptr);
-    if (b2 > *bytes) *bytes = b2;
-    if (b3 > *bytes) *bytes = b3;
-    // any kp: nt_neg + nt_pos <= nv/32 + 2
-    const size_t worst = carve_instance(nullptr, grid->nx, grid->nv + 64, (grid->nv + 64) / 2, p, nullptr);
-    if (worst > *bytes) *bytes = worst;
+    // the v-tile count depends on where v changes sign (kp): at most
+    // nv/32 + 2 tiles; size for the worst case so the query needs no v
+    size_t best = 0;
+    const int kps[3] = {0, grid->nv, grid->nv / 2 + 1 <= grid->nv ? grid->nv / 2 + 1 : grid->nv};
+    for (int q = 0; q < 3; ++q) {
+        const size_t b = carve_instance(nullptr, grid->nx, grid->nv, kps[q], p, nullptr);
+        if (b > best) best = b;
+    }
+    const size_t worst =
+        carve_instance(nullptr, grid->nx, grid->nv + 64, (grid->nv + 64) / 2, p, nullptr);
+    *bytes = worst > best ? worst : best;
     return KEQ_OK;
 }
 
@@ -1251,13 +1053,21 @@ keq_status keq_implicit_plan_create(const keq_instance* insts, int32_t n,
     if (plan_ws_bytes < plan_bytes(n, max_iter)) return KEQ_ERR_WORKSPACE;
 
     keq_plan* plan = new keq_plan();
+    plan->kind = KEQ_PLAN_IMPLICIT;
     plan->n_inst = n;
     plan->device = dev_of_buffers;
-    plan->host_inst.resize(n);
-    plan->tile_off.resize(n + 1);
-    plan->rb_off.resize(n + 1);
+    plan->inst_bytes = sizeof(ImpInst);
+    plan->off_f_in = offsetof(ImpInst, f_in);
+    plan->off_f_out = offsetof(ImpInst, f_out);
+    plan->kernel = (const void*)keq::implicit_step_kernel;
+    plan->smem = keq::kSmemBytes;
+    plan->threads = keq::kThreads;
+    plan->host_inst.resize(sizeof(ImpInst) * (size_t)n);
+    std::vector<ImpInst> host_inst(n);
+    std::vector<long long> tile_off(n + 1), rb_off(n + 1);
     long long toff = 0, roff = 0;
     std::vector<double> vh;
+    cudaError_t e = cudaSuccess;
     for (int b = 0; b < n; ++b) {
         const keq_instance& in = insts[b];
         const keq_implicit_params p = normalized(params[per_instance_params ? b : 0]);
@@ -1294,6 +1104,7 @@ keq_status keq_implicit_plan_create(const keq_instance* insts, int32_t n,
         ImpInst I{};
         I.nx = nx; I.nv = nv; I.n_inner = d.n_inner; I.kp = kp;
         I.nt_neg = d.nt_neg; I.nvt = d.nvt; I.nchunks = d.nchunks; I.nrb = d.nrb;
+        I.rows = d.rows;
         I.tile_off = toff; I.rb_off = roff;
         I.dx = in.grid.dx; I.dv = in.grid.dv; I.dt = in.dt; I.tau_tilde = in.tau_tilde;
         I.dtdx = in.dt / in.grid.dx;
@@ -1305,14 +1116,27 @@ keq_status keq_implicit_plan_create(const keq_instance* insts, int32_t n,
         I.aa_alpha_max = p.aa_alpha_max;
         I.v = in.grid.v; I.f_in = in.f_in; I.f_out = in.f_out; I.stats = in.stats;
         carve_instance(in.workspace, nx, nv, kp, p, &I);
-        plan->host_inst[b] = I;
-        plan->tile_off[b] = toff;
-        plan->rb_off[b] = roff;
+        // look-back flags start at epoch 0 (never current): a workspace that
+        // held another plan cannot leave flags that look published
+        e = cudaMemsetAsync(I.flag, 0, sizeof(unsigned long long) * (size_t)d.nvt * d.nchunks, s);
+        if (e != cudaSuccess) {
+            keq_internal_set_cuda_error(e);
+            delete plan;
+            return KEQ_ERR_CUDA;
+        }
+        host_inst[b] = I;
+        tile_off[b] = toff;
+        rb_off[b] = roff;
         toff += (long long)d.nvt * d.nchunks;
         roff += d.nrb;
     }
-    plan->tile_off[n] = toff;
-    plan->rb_off[n] = roff;
+    tile_off[n] = toff;
+    rb_off[n] = roff;
+    memcpy(plan->host_inst.data(), host_inst.data(), sizeof(ImpInst) * (size_t)n);
+    if (toff >= (long long)0xffffffffll) {
+        delete plan;
+        return KEQ_ERR_INVALID;  // tile tickets are 32-bit
+    }
 
     Carve c{static_cast<char*>(plan_ws), 0};
     PlanDev* dev = c.take<PlanDev>(1);
@@ -1321,7 +1145,8 @@ keq_status keq_implicit_plan_create(const keq_instance* insts, int32_t n,
     long long* droff = c.take<long long>(n + 1);
     unsigned* tickets = c.take<unsigned>(max_iter + 1);
     PlanDev h{};
-    h.spin_limit = kSpinLimit;
+    h.head.spin_limit = kSpinLimit;
+    h.head.seq = 0ull;
     h.n_inst = n;
     h.max_iter = max_iter;
     h.total_tiles = toff;
@@ -1332,16 +1157,15 @@ keq_status keq_implicit_plan_create(const keq_instance* insts, int32_t n,
     h.tickets = tickets;
     plan->dev = dev;
     plan->dev_inst = dinst;
-    cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = cudaMemcpyAsync(dev, &h, sizeof(h), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(dinst, plan->host_inst.data(), sizeof(ImpInst) * n,
+        e = cudaMemcpyAsync(dinst, host_inst.data(), sizeof(ImpInst) * n,
                             cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(dtoff, plan->tile_off.data(), sizeof(long long) * (n + 1),
+        e = cudaMemcpyAsync(dtoff, tile_off.data(), sizeof(long long) * (n + 1),
                             cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(droff, plan->rb_off.data(), sizeof(long long) * (n + 1),
+        e = cudaMemcpyAsync(droff, rb_off.data(), sizeof(long long) * (n + 1),
                             cudaMemcpyHostToDevice, s);
     // stats start from zero totals
     if (e == cudaSuccess)
@@ -1353,124 +1177,12 @@ keq_status keq_implicit_plan_create(const keq_instance* insts, int32_t n,
         delete plan;
         return KEQ_ERR_CUDA;
     }
-    int dev_id = 0, sms = 0, occ = 0;
-    cudaGetDevice(&dev_id);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id);
-    cudaFuncSetAttribute(keq::implicit_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)keq::kSmemBytes);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, keq::implicit_step_kernel, kThreads,
-                                                  keq::kSmemBytes);
-    if (occ < 1 || sms < 1) {
+    const keq_status gs = keq_internal_plan_grid(plan);
+    if (gs != KEQ_OK) {
         delete plan;
-        return KEQ_ERR_UNSUPPORTED;
+        return gs;
     }
-    // every resident CTA takes part: work items are strided over all warps
-    plan->grid = sms * occ;
     *plan_out = plan;
-    return KEQ_OK;
-}
-
-keq_status keq_plan_set_buffers(keq_plan* plan, const double* const* f_in, double* const* f_out,
-                                keq_stream_t stream) {
-    if (!plan || !f_in || !f_out) return KEQ_ERR_INVALID;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    for (int b = 0; b < plan->n_inst; ++b) {
-        if (!f_in[b] || !f_out[b] || f_in[b] == f_out[b]) return KEQ_ERR_INVALID;
-        plan->host_inst[b].f_in = f_in[b];
-        plan->host_inst[b].f_out = f_out[b];
-    }
-    cudaError_t e = cudaMemcpyAsync(plan->dev_inst, plan->host_inst.data(),
-                                    sizeof(ImpInst) * plan->n_inst, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) {
-        keq_internal_set_cuda_error(e);
-        return KEQ_ERR_CUDA;
-    }
-    return KEQ_OK;
-}
-
-keq_status keq_plan_step(keq_plan* plan, int32_t n_steps, int32_t parity, keq_stream_t stream) {
-    if (!plan || n_steps < 0) return KEQ_ERR_INVALID;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    if (cudaSetDevice(plan->device) != cudaSuccess) {
-        keq_internal_set_cuda_error(cudaGetLastError());
-        return KEQ_ERR_CUDA;
-    }
-    for (int k = 0; k < n_steps; ++k) {
-        int swap_io = ((parity + k) & 1);
-        // fresh barrier and error word for this launch (bar.count, bar.gen, err)
-        cudaError_t me = cudaMemsetAsync(plan->dev, 0, offsetof(PlanDev, err_sticky), s);
-        if (me != cudaSuccess) {
-            keq_internal_set_cuda_error(me);
-            return KEQ_ERR_CUDA;
-        }
-        void* args[] = {&plan->dev, &swap_io};
-        cudaError_t e = cudaLaunchCooperativeKernel((const void*)keq::implicit_step_kernel,
-                                                    dim3(plan->grid), dim3(keq::kThreads), args,
-                                                    keq::kSmemBytes, s);
-        if (e != cudaSuccess) {
-            keq_internal_set_cuda_error(e);
-            return KEQ_ERR_CUDA;
-        }
-    }
-    return KEQ_OK;
-}
-
-void keq_plan_destroy(keq_plan* plan) { delete plan; }
-
-keq_status keq_plan_set_trace(keq_plan* plan, unsigned long long* trace, int32_t iters,
-                              keq_stream_t stream) {
-    if (!plan || iters < 0 || (iters > 0 && !trace)) return KEQ_ERR_INVALID;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    keq::PlanDev* d = plan->dev;
-    unsigned long long* tp = iters > 0 ? trace : nullptr;
-    cudaError_t e = cudaMemcpyAsync(&d->trace, &tp, sizeof(tp), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(&d->trace_iters, &iters, sizeof(int), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) {
-        keq_internal_set_cuda_error(e);
-        return KEQ_ERR_CUDA;
-    }
-    return KEQ_OK;
-}
-
-keq_status keq_plan_error(keq_plan* plan, keq_stream_t stream, int32_t* err_bits) {
-    if (!plan || !err_bits) return KEQ_ERR_INVALID;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    int v = 0;
-    cudaError_t e =
-        cudaMemcpyAsync(&v, &plan->dev->err_sticky, sizeof(int), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) {
-        keq_internal_set_cuda_error(e);
-        return KEQ_ERR_CUDA;
-    }
-    *err_bits = v;
-    return KEQ_OK;
-}
-
-keq_status keq_plan_reset(keq_plan* plan, keq_stream_t stream) {
-    if (!plan) return KEQ_ERR_INVALID;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    cudaError_t e = cudaMemsetAsync(plan->dev, 0, offsetof(PlanDev, spin_limit), s);
-    if (e != cudaSuccess) {
-        keq_internal_set_cuda_error(e);
-        return KEQ_ERR_CUDA;
-    }
-    return KEQ_OK;
-}
-
-keq_status keq_plan_set_spin_limit(keq_plan* plan, unsigned long long limit, keq_stream_t stream) {
-    if (!plan) return KEQ_ERR_INVALID;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const unsigned long long v = limit == 0ull ? 0ull : limit;
-    cudaError_t e = cudaMemcpyAsync(&plan->dev->spin_limit, &v, sizeof(v), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) {
-        keq_internal_set_cuda_error(e);
-        return KEQ_ERR_CUDA;
-    }
     return KEQ_OK;
 }
 

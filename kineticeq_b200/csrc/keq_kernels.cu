@@ -143,44 +143,209 @@ __device__ __forceinline__ void m3inv(const double* M, double* Mi) {
     Mi[6] = c02 * id; Mi[7] = c12 * id; Mi[8] = c22 * id;
 }
 
-// Block Thomas, one thread per system; C' and D' in the workspace.
-__global__ void __launch_bounds__(64) block_thomas_kernel(const double* __restrict__ A,
-                                                          const double* __restrict__ Bm,
-                                                          const double* __restrict__ C,
-                                                          const double* __restrict__ D,
-                                                          double* __restrict__ X, int n, int batch,
-                                                          double* __restrict__ ws) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= batch) return;
+// Partition method for batched 3x3 block-tridiagonal systems
+//   A_i x_{i-1} + B_i x_i + C_i x_{i+1} = D_i,   i = 0 .. n-1 (A_0, C_{n-1} ignored).
+// Rows are cut into K chunks of L rows.  Per chunk (one thread), the rows
+// s..e-1 before the chunk's last row e are eliminated by block Thomas with
+// the chunk's two interface unknowns xi_{k-1} = x_{s-1} and xi_k = x_e moved
+// to the right-hand side, giving x_i = y_i + P_i xi_{k-1} + Q_i xi_k.  The
+// chunks' last rows then form a K-row block-tridiagonal system in the xi,
+// solved by parallel cyclic reduction in one CTA per system; a last pass
+// recovers every x_i.  Singular 3x3 pivots (|det| < 1e-30) contribute a zero
+// inverse, the convention of lo_blocktridiag/block_tridiag_kernel.cu:32-68.
+struct BtGeo {
+    int L, K;
+};
+__host__ __device__ inline BtGeo bt_geo(int n) {
+    BtGeo g;
+    int L = (n + 127) / 128;
+    if (L < 8) L = 8;
+    g.L = L;
+    g.K = (n + L - 1) / L;
+    return g;
+}
+constexpr int kBtRep = 21;  // y (3) | P (3x3) | Q (3x3) per row
+
+__global__ void __launch_bounds__(64) bt_local_kernel(const double* __restrict__ A,
+                                                      const double* __restrict__ Bm,
+                                                      const double* __restrict__ C,
+                                                      const double* __restrict__ D, int n,
+                                                      int batch, double* __restrict__ rep,
+                                                      double* __restrict__ cpw) {
+    const BtGeo G = bt_geo(n);
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)batch * G.K) return;
+    const int b = (int)(t / G.K), k = (int)(t % G.K);
+    const int s = k * G.L;
+    const int e = (s + G.L < n ? s + G.L : n) - 1;
     const size_t mo = (size_t)b * n * 9, vo = (size_t)b * n * 3;
-    double* Cp = ws + (size_t)b * n * 12;
-    double* Dp = Cp + (size_t)n * 9;
-    double Mi[9], T9[9], t3[3], M[9], rhs[3];
-    for (int i = 0; i < n; ++i) {
-        if (i == 0) {
-#pragma unroll
-            for (int k = 0; k < 9; ++k) M[k] = Bm[mo + k];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) rhs[k] = D[vo + k];
+    double* R = rep + (size_t)b * n * kBtRep;
+    double* Cp = cpw + (size_t)b * n * 9;
+    const int nloc = e - s;  // rows s..e-1
+    // forward sweep: R'_i = M_i^-1 (R_i - A_i R'_{i-1}), C'_i = M_i^-1 C_i
+    for (int r = 0; r < nloc; ++r) {
+        const int i = s + r;
+        const double* Ai = A + mo + 9 * (size_t)i;
+        double M[9], ry[3], rP[9], rQ[9];
+        if (r == 0) {
+            for (int q = 0; q < 9; ++q) M[q] = Bm[mo + 9 * (size_t)i + q];
+            for (int q = 0; q < 3; ++q) ry[q] = D[vo + 3 * (size_t)i + q];
+            for (int q = 0; q < 9; ++q) rP[q] = (k == 0) ? 0.0 : -Ai[q];
+            for (int q = 0; q < 9; ++q) rQ[q] = 0.0;
         } else {
-            m3mul(A + mo + 9 * (size_t)i, Cp + 9 * (size_t)(i - 1), T9);
-#pragma unroll
-            for (int k = 0; k < 9; ++k) M[k] = Bm[mo + 9 * (size_t)i + k] - T9[k];
-            m3vec(A + mo + 9 * (size_t)i, Dp + 3 * (size_t)(i - 1), t3);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) rhs[k] = D[vo + 3 * (size_t)i + k] - t3[k];
+            double T9[9], t3[3];
+            m3mul(Ai, Cp + 9 * (size_t)(i - 1), T9);
+            for (int q = 0; q < 9; ++q) M[q] = Bm[mo + 9 * (size_t)i + q] - T9[q];
+            const double* Rp = R + kBtRep * (size_t)(i - 1);
+            m3vec(Ai, Rp, t3);
+            for (int q = 0; q < 3; ++q) ry[q] = D[vo + 3 * (size_t)i + q] - t3[q];
+            m3mul(Ai, Rp + 3, T9);
+            for (int q = 0; q < 9; ++q) rP[q] = -T9[q];
+            m3mul(Ai, Rp + 12, T9);
+            for (int q = 0; q < 9; ++q) rQ[q] = -T9[q];
         }
+        if (r == nloc - 1)
+            for (int q = 0; q < 9; ++q) rQ[q] -= C[mo + 9 * (size_t)i + q];
+        double Mi[9];
         m3inv(M, Mi);
-        if (i < n - 1) m3mul(Mi, C + mo + 9 * (size_t)i, Cp + 9 * (size_t)i);
-        m3vec(Mi, rhs, Dp + 3 * (size_t)i);
+        double* Ro = R + kBtRep * (size_t)i;
+        m3vec(Mi, ry, Ro);
+        m3mul(Mi, rP, Ro + 3);
+        m3mul(Mi, rQ, Ro + 12);
+        if (r < nloc - 1) m3mul(Mi, C + mo + 9 * (size_t)i, Cp + 9 * (size_t)i);
     }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) X[vo + 3 * (size_t)(n - 1) + k] = Dp[3 * (size_t)(n - 1) + k];
-    for (int i = n - 2; i >= 0; --i) {
-        m3vec(Cp + 9 * (size_t)i, X + vo + 3 * (size_t)(i + 1), t3);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) X[vo + 3 * (size_t)i + k] = Dp[3 * (size_t)i + k] - t3[k];
+    // backward sweep: x_i = R'_i - C'_i x_{i+1}
+    for (int r = nloc - 2; r >= 0; --r) {
+        const int i = s + r;
+        double* Ro = R + kBtRep * (size_t)i;
+        const double* Rn = R + kBtRep * (size_t)(i + 1);
+        const double* Ci = Cp + 9 * (size_t)i;
+        double t3[3], T9[9];
+        m3vec(Ci, Rn, t3);
+        for (int q = 0; q < 3; ++q) Ro[q] -= t3[q];
+        m3mul(Ci, Rn + 3, T9);
+        for (int q = 0; q < 9; ++q) Ro[3 + q] -= T9[q];
+        m3mul(Ci, Rn + 12, T9);
+        for (int q = 0; q < 9; ++q) Ro[12 + q] -= T9[q];
     }
+    // the chunk's last row is its interface unknown: y = 0, P = 0, Q = I
+    double* Re = R + kBtRep * (size_t)e;
+    for (int q = 0; q < kBtRep; ++q) Re[q] = 0.0;
+    Re[12] = Re[16] = Re[20] = 1.0;
+}
+
+struct BtRed {
+    double al[9], be[9], ga[9], de[3];
+};
+
+__global__ void __launch_bounds__(128) bt_reduced_kernel(const double* __restrict__ A,
+                                                         const double* __restrict__ Bm,
+                                                         const double* __restrict__ C,
+                                                         const double* __restrict__ D, int n,
+                                                         const double* __restrict__ rep,
+                                                         double* __restrict__ xi) {
+    extern __shared__ __align__(16) unsigned char bt_smem[];
+    const BtGeo G = bt_geo(n);
+    const int b = blockIdx.x, K = G.K;
+    BtRed* buf[2] = {reinterpret_cast<BtRed*>(bt_smem), reinterpret_cast<BtRed*>(bt_smem) + K};
+    const size_t mo = (size_t)b * n * 9, vo = (size_t)b * n * 3;
+    const double* R = rep + (size_t)b * n * kBtRep;
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        const int s = k * G.L;
+        const int e = (s + G.L < n ? s + G.L : n) - 1;
+        const double* Ae = A + mo + 9 * (size_t)e;
+        const double* Be = Bm + mo + 9 * (size_t)e;
+        const double* Ce = C + mo + 9 * (size_t)e;
+        double pm[kBtRep], nx_[kBtRep];
+        for (int q = 0; q < kBtRep; ++q) pm[q] = 0.0;
+        if (e > s) {
+            for (int q = 0; q < kBtRep; ++q) pm[q] = R[kBtRep * (size_t)(e - 1) + q];
+        } else {
+            pm[3] = pm[7] = pm[11] = 1.0;  // x_{e-1} = xi_{k-1}
+        }
+        for (int q = 0; q < kBtRep; ++q) nx_[q] = 0.0;
+        const bool has_next = k + 1 < K;
+        if (has_next)
+            for (int q = 0; q < kBtRep; ++q) nx_[q] = R[kBtRep * (size_t)(e + 1) + q];
+        double Aeff[9], Ceff[9];
+        for (int q = 0; q < 9; ++q) {
+            Aeff[q] = (e == 0) ? 0.0 : Ae[q];
+            Ceff[q] = has_next ? Ce[q] : 0.0;
+        }
+        BtRed r;
+        double T9[9], U9[9], t3[3], u3[3];
+        m3mul(Aeff, pm + 3, r.al);
+        m3mul(Aeff, pm + 12, T9);
+        m3mul(Ceff, nx_ + 3, U9);
+        for (int q = 0; q < 9; ++q) r.be[q] = Be[q] + T9[q] + U9[q];
+        m3mul(Ceff, nx_ + 12, r.ga);
+        m3vec(Aeff, pm, t3);
+        m3vec(Ceff, nx_, u3);
+        for (int q = 0; q < 3; ++q) r.de[q] = D[vo + 3 * (size_t)e + q] - t3[q] - u3[q];
+        buf[0][k] = r;
+    }
+    __syncthreads();
+    int cur = 0;
+    for (int sd = 1; sd < K; sd <<= 1) {
+        for (int k = threadIdx.x; k < K; k += blockDim.x) {
+            const BtRed& me = buf[cur][k];
+            BtRed nw = me;
+            double bi[9], e1[9], T9[9], t3[3];
+            if (k - sd >= 0) {
+                const BtRed& lo = buf[cur][k - sd];
+                m3inv(lo.be, bi);
+                m3mul(me.al, bi, e1);
+                m3mul(e1, lo.al, T9);
+                for (int q = 0; q < 9; ++q) nw.al[q] = -T9[q];
+                m3mul(e1, lo.ga, T9);
+                for (int q = 0; q < 9; ++q) nw.be[q] -= T9[q];
+                m3vec(e1, lo.de, t3);
+                for (int q = 0; q < 3; ++q) nw.de[q] -= t3[q];
+            } else {
+                for (int q = 0; q < 9; ++q) nw.al[q] = 0.0;
+            }
+            if (k + sd < K) {
+                const BtRed& hi = buf[cur][k + sd];
+                m3inv(hi.be, bi);
+                m3mul(me.ga, bi, e1);
+                m3mul(e1, hi.ga, T9);
+                for (int q = 0; q < 9; ++q) nw.ga[q] = -T9[q];
+                m3mul(e1, hi.al, T9);
+                for (int q = 0; q < 9; ++q) nw.be[q] -= T9[q];
+                m3vec(e1, hi.de, t3);
+                for (int q = 0; q < 3; ++q) nw.de[q] -= t3[q];
+            } else {
+                for (int q = 0; q < 9; ++q) nw.ga[q] = 0.0;
+            }
+            buf[cur ^ 1][k] = nw;
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        double bi[9];
+        m3inv(buf[cur][k].be, bi);
+        m3vec(bi, buf[cur][k].de, xi + ((size_t)b * K + k) * 3);
+    }
+}
+
+__global__ void __launch_bounds__(128) bt_recover_kernel(int n, int batch,
+                                                         const double* __restrict__ rep,
+                                                         const double* __restrict__ xi,
+                                                         double* __restrict__ X) {
+    const BtGeo G = bt_geo(n);
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)batch * n) return;
+    const int b = (int)(t / n), i = (int)(t % n);
+    const int k = i / G.L;
+    const double* R = rep + ((size_t)b * n + i) * kBtRep;
+    const double* xl = xi + ((size_t)b * G.K + (k > 0 ? k - 1 : 0)) * 3;
+    const double* xr = xi + ((size_t)b * G.K + k) * 3;
+    double out[3], a3[3], c3[3];
+    m3vec(R + 3, xl, a3);
+    m3vec(R + 12, xr, c3);
+    for (int q = 0; q < 3; ++q) out[q] = R[q] + (k > 0 ? a3[q] : 0.0) + c3[q];
+    for (int q = 0; q < 3; ++q) X[((size_t)b * n + i) * 3 + q] = out[q];
 }
 
 // ---- Maxwellian of per-row moments -----------------------------------------
@@ -334,7 +499,9 @@ keq_status keq_gtsv_strided_inplace(const double* dl, const double* d, const dou
 
 keq_status keq_block_tridiag_workspace_size(int32_t n, int32_t batch, size_t* bytes) {
     if (!bytes || n < 0 || batch < 0) return KEQ_ERR_INVALID;
-    *bytes = sizeof(double) * 12 * (size_t)(n > 0 ? n : 1) * (size_t)(batch > 0 ? batch : 1);
+    const size_t nn = (size_t)(n > 0 ? n : 1), bb = (size_t)(batch > 0 ? batch : 1);
+    const keq::BtGeo G = keq::bt_geo(n > 0 ? n : 1);
+    *bytes = sizeof(double) * (nn * bb * (keq::kBtRep + 9) + (size_t)G.K * bb * 3) + 256;
     return KEQ_OK;
 }
 
@@ -349,8 +516,19 @@ keq_status keq_block_tridiag_solve(const double* A, const double* B, const doubl
     keq_block_tridiag_workspace_size(n, batch, &need);
     if (workspace_bytes < need || reinterpret_cast<uintptr_t>(workspace) % 8)
         return KEQ_ERR_WORKSPACE;
-    keq::block_thomas_kernel<<<(batch + 63) / 64, 64, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-        A, B, C, D, X, n, batch, static_cast<double*>(workspace));
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const keq::BtGeo G = keq::bt_geo(n);
+    double* rep = static_cast<double*>(workspace);
+    double* cpw = rep + (size_t)n * batch * keq::kBtRep;
+    double* xi = cpw + (size_t)n * batch * 9;
+    const long long nloc = (long long)batch * G.K;
+    keq::bt_local_kernel<<<(unsigned)((nloc + 63) / 64), 64, 0, s>>>(A, B, C, D, n, batch, rep, cpw);
+    const size_t smem = 2 * sizeof(keq::BtRed) * (size_t)G.K;
+    cudaFuncSetAttribute(keq::bt_reduced_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    keq::bt_reduced_kernel<<<batch, 128, smem, s>>>(A, B, C, D, n, rep, xi);
+    const long long nrow = (long long)batch * n;
+    keq::bt_recover_kernel<<<(unsigned)((nrow + 127) / 128), 128, 0, s>>>(n, batch, rep, xi, X);
     return launch_status();
 }
 

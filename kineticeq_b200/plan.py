@@ -27,9 +27,11 @@ _STATS_DTYPE = np.dtype([
 assert _STATS_DTYPE.itemsize == N.STATS_BYTES
 
 
-def implicit_params_struct(sp=None, fixed_iters: int = 0, **kw) -> N.ImplicitParams:
+def implicit_params_struct(sp=None, fixed_iters: int = 0, tile_rows: int = 0,
+                           **kw) -> N.ImplicitParams:
     """implicit.Params (or keywords) -> keq_implicit_params; the clamps of
-    bgk1d_implicit_cuda_kernel.py:49-65 are applied inside the library."""
+    bgk1d_implicit_cuda_kernel.py:49-65 are applied inside the library.
+    tile_rows (8/16/24/32, 0 = default) is this backend's tile height."""
     g = (lambda k, d: kw[k] if k in kw else getattr(sp, k, d))
     conv = str(g("conv_type", "f")).lower()
     if conv not in ("f", "w"):
@@ -38,7 +40,8 @@ def implicit_params_struct(sp=None, fixed_iters: int = 0, **kw) -> N.ImplicitPar
         int(g("picard_iter", 16)), float(g("picard_tol", 1e-4)), float(g("abs_tol", 1e-16)),
         1 if conv == "w" else 0, int(bool(g("aa_enable", False))), int(g("aa_m", 6)),
         float(g("aa_beta", 1.0)), int(g("aa_stride", 1)), int(g("aa_start_iter", 2)),
-        float(g("aa_reg", 1e-10)), float(g("aa_alpha_max", 50.0)), int(fixed_iters))
+        float(g("aa_reg", 1e-10)), float(g("aa_alpha_max", 50.0)), int(fixed_iters),
+        int(tile_rows))
 
 
 @dataclass
@@ -134,8 +137,36 @@ class StatsSnapshot:
         return self._vals
 
 
-class ImplicitPlan:
-    """Batched implicit Picard stepping of independent instances."""
+def holo_params_struct(sp=None, fixed_ho_iters: int = 0, fixed_lo_iters: int = 0,
+                       **kw) -> N.HoloParams:
+    """holo.Params (or keywords) -> keq_holo_params (holo.py:5-13 plus the
+    hidden SVdown flag read at bgk1d_holo_cuda_kernel.py:443)."""
+    g = (lambda k, d: kw[k] if k in kw else getattr(sp, k, d))
+    return N.HoloParams(
+        int(g("ho_iter", 8)), float(g("ho_tol", 1e-4)), float(g("ho_abs_tol", 1e-12)),
+        int(g("lo_iter", 16)), float(g("lo_tol", 1e-4)), float(g("lo_abs_tol", 1e-12)),
+        int(bool(g("Con_Terms_do", True))), int(bool(g("flux_consistency_do", True))),
+        int(bool(g("SVdown", False))), int(fixed_ho_iters), int(fixed_lo_iters))
+
+
+class _StepPlan:
+    """A list of independent instances stepped together by one persistent
+    kernel launch per time step (keq_plan of the C ABI)."""
+
+    _kind = "step"
+    _ptype = None
+
+    def _to_struct(self, p):
+        raise NotImplementedError
+
+    def _ws_query(self, lib, grid, p, nbytes):
+        raise NotImplementedError
+
+    def _plan_ws_query(self, lib, inst, n, parr, per, nbytes):
+        raise NotImplementedError
+
+    def _create(self, lib, inst, n, parr, per, ws, nws, sh, handle):
+        raise NotImplementedError
 
     def __init__(self, specs: Sequence[InstanceSpec], params, stream=None):
         lib = N.load()
@@ -144,8 +175,7 @@ class ImplicitPlan:
         plist = list(params) if isinstance(params, (list, tuple)) else [params]
         if len(plist) not in (1, len(specs)):
             raise ValueError("params: one record or one per instance")
-        pstructs = [p if isinstance(p, N.ImplicitParams) else implicit_params_struct(p)
-                    for p in plist]
+        pstructs = [p if isinstance(p, self._ptype) else self._to_struct(p) for p in plist]
         self.device = specs[0].a.device
         self.specs = list(specs)
         self.n = len(specs)
@@ -164,24 +194,21 @@ class ImplicitPlan:
             p = pstructs[i if len(pstructs) > 1 else 0]
             grid = N.Grid(s.nx, s.nv, float(s.dx), float(s.dv), s.v.data_ptr())
             nbytes = C.c_size_t(0)
-            N.check(lib.keq_implicit_instance_workspace_size(C.byref(grid), C.byref(p),
-                                                             C.byref(nbytes)), "workspace query")
+            N.check(self._ws_query(lib, grid, p, nbytes), "workspace query")
             ws = torch.empty((max(int(nbytes.value), 256),), dtype=torch.uint8,
                              device=self.device)
             self._ws.append(ws)
             inst[i] = N.Instance(grid, float(s.dt), float(s.tau_tilde), s.a.data_ptr(),
                                  s.b.data_ptr(), self.stats_dev[i].data_ptr(), ws.data_ptr())
-        parr = (N.ImplicitParams * len(pstructs))(*pstructs)
+        parr = (self._ptype * len(pstructs))(*pstructs)
         per = 1 if len(pstructs) > 1 else 0
         nbytes = C.c_size_t(0)
-        N.check(lib.keq_implicit_plan_workspace_size(inst, self.n, parr, per, C.byref(nbytes)),
-                "plan workspace query")
+        N.check(self._plan_ws_query(lib, inst, self.n, parr, per, nbytes), "plan workspace query")
         self._plan_ws = torch.empty((max(int(nbytes.value), 256),), dtype=torch.uint8,
                                     device=self.device)
         handle = C.c_void_p(0)
-        N.check(lib.keq_implicit_plan_create(inst, self.n, parr, per,
-                                             self._plan_ws.data_ptr(), self._plan_ws.numel(),
-                                             sh, C.byref(handle)), "plan creation")
+        N.check(self._create(lib, inst, self.n, parr, per, self._plan_ws.data_ptr(),
+                             self._plan_ws.numel(), sh, handle), "plan creation")
         self._h = handle
         self._lib = lib
         self.parity = 0  # 0: newest state in `a`, 1: in `b`
@@ -190,7 +217,7 @@ class ImplicitPlan:
 
     def step(self, n_steps: int = 1) -> None:
         N.check(self._lib.keq_plan_step(self._h, int(n_steps), int(self.parity),
-                                        N.stream_handle(self._stream)), "implicit step")
+                                        N.stream_handle(self._stream)), f"{self._kind} step")
         self.parity = (self.parity + int(n_steps)) & 1
 
     def snapshot(self) -> StatsSnapshot:
@@ -228,15 +255,16 @@ class ImplicitPlan:
         return buf
 
     def trace_phases(self):
-        """Per-iteration (pass1_us, barrier_us, pass2_us) of the last step."""
+        """Per-iteration (pass_us, gap_to_next_pass_us) of the last step."""
         import numpy as np
 
         t = self._trace.cpu().numpy().view(np.uint64).astype(np.float64)
         out = []
-        for row in t:
+        for m, row in enumerate(t):
             if row[1] == 0:
                 break
-            out.append(((row[1] - row[0]) / 1e3, (row[2] - row[1]) / 1e3, (row[3] - row[2]) / 1e3))
+            nxt = t[m + 1][0] if m + 1 < len(t) and t[m + 1][1] != 0 else row[1]
+            out.append(((row[1] - row[0]) / 1e3, (nxt - row[1]) / 1e3))
         return out
 
     def reset_trace(self) -> None:
@@ -260,6 +288,49 @@ class ImplicitPlan:
             self.close()
         except Exception:
             pass
+
+
+class ImplicitPlan(_StepPlan):
+    """Batched implicit Picard stepping of independent instances."""
+
+    _kind = "implicit"
+    _ptype = N.ImplicitParams
+
+    def _to_struct(self, p):
+        return implicit_params_struct(p)
+
+    def _ws_query(self, lib, grid, p, nbytes):
+        return lib.keq_implicit_instance_workspace_size(C.byref(grid), C.byref(p), C.byref(nbytes))
+
+    def _plan_ws_query(self, lib, inst, n, parr, per, nbytes):
+        return lib.keq_implicit_plan_workspace_size(inst, n, parr, per, C.byref(nbytes))
+
+    def _create(self, lib, inst, n, parr, per, ws, nws, sh, handle):
+        return lib.keq_implicit_plan_create(inst, n, parr, per, ws, nws, sh, C.byref(handle))
+
+    def moments(self, i: int) -> torch.Tensor:
+        """(3, nx) view of instance i's current W = (n, nu, T) (workspace head)."""
+        nx = self.specs[i].nx
+        return self._ws[i][: 3 * nx * 8].view(torch.float64).view(3, nx)
+
+
+class HoloPlan(_StepPlan):
+    """Batched HOLO stepping of independent instances."""
+
+    _kind = "holo"
+    _ptype = N.HoloParams
+
+    def _to_struct(self, p):
+        return holo_params_struct(p)
+
+    def _ws_query(self, lib, grid, p, nbytes):
+        return lib.keq_holo_instance_workspace_size(C.byref(grid), C.byref(p), C.byref(nbytes))
+
+    def _plan_ws_query(self, lib, inst, n, parr, per, nbytes):
+        return lib.keq_holo_plan_workspace_size(inst, n, parr, per, C.byref(nbytes))
+
+    def _create(self, lib, inst, n, parr, per, ws, nws, sh, handle):
+        return lib.keq_holo_plan_create(inst, n, parr, per, ws, nws, sh, C.byref(handle))
 
 
 def grid_of(nx: int, nv: int, Lx: float = 1.0, v_max: float = 10.0, device="cuda"):

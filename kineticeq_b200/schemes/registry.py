@@ -9,23 +9,12 @@ from __future__ import annotations
 from typing import Any, Callable
 
 from ..api.config import Backend, Config, Model, Scheme
-from . import bgk1d_implicit
-
-Stepper = Callable[[int], None]
-StepperBuilder = Callable[[Config, Any], Stepper]
+from . import bgk1d_holo, bgk1d_implicit
 
 _FACTORIES: dict = {
     (Model.BGK1D1V, Scheme.IMPLICIT, Backend.CUDA_KERNEL): bgk1d_implicit.build_stepper,
+    (Model.BGK1D1V, Scheme.HOLO, Backend.CUDA_KERNEL): bgk1d_holo.build_stepper,
 }
-
-
-def _holo_builder(cfg, state):
-    from . import bgk1d_holo
-
-    return bgk1d_holo.build_stepper(cfg, state)
-
-
-_FACTORIES[(Model.BGK1D1V, Scheme.HOLO, Backend.CUDA_KERNEL)] = _holo_builder
 
 
 def build_stepper(cfg: Config, state: Any) -> Stepper:

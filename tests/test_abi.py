@@ -32,7 +32,7 @@ def test_status_strings(lib):
 
 def test_workspace_queries_validate(lib):
     g = N.Grid(256, 128, 1 / 255, 20 / 127, 0)
-    p = N.ImplicitParams(64, 1e-10, 1e-16, 0, 0, 5, 1.0, 1, 2, 1e-10, 50.0, 0)
+    p = N.ImplicitParams(64, 1e-10, 1e-16, 0, 0, 5, 1.0, 1, 2, 1e-10, 50.0, 0, 0)
     nb = C.c_size_t(0)
     assert lib.keq_implicit_instance_workspace_size(C.byref(g), C.byref(p), C.byref(nb)) == 0
     assert nb.value > 256 * 4 * 8
@@ -47,3 +47,4 @@ def test_workspace_queries_validate(lib):
     assert lib.keq_gtsv_strided_inplace(0, 0, 0, 0, 5, 3, 0, 0, 0) == 1
     assert lib.keq_block_tridiag_workspace_size(10, 2, C.byref(nb)) == 0
     assert lib.keq_moments_n_nu_T(0, 0, 4, 4, 1.0, 0, 0, 0, 0) == 1
+
