@@ -241,6 +241,24 @@ keq_status keq_gtsv_strided_inplace(const double* dl, const double* d, const dou
                                     double* B, int32_t n, int32_t batch, void* workspace,
                                     size_t workspace_bytes, keq_stream_t stream);
 
+/* The same solve as keq_gtsv_strided_inplace, for callers that cannot
+ * allocate device memory and so cannot pass a workspace (a binding that only
+ * forwards the operation's own tensors, or a host that must not call
+ * cudaMalloc).  It allocates nothing: its scratch is a fixed array inside the
+ * library, KEQ_GTSV_NOALLOC_MAX_ELEMS doubles (16 MiB) on every GPU that
+ * loads the library, held until the process exits.  n * batch above that
+ * limit returns KEQ_ERR_CAPACITY.  The first call on a device looks the
+ * array's device address up (with that device current) and caches it; make
+ * that first call before any stream capture.  All calls share the one array,
+ * so two calls that may overlap on the GPU (different streams, no ordering)
+ * race on it: order them on one stream.  It keeps the last call's contents,
+ * which is harmless here because the kernel writes every scratch element it
+ * reads.  This entry point has no counterpart in the reference. */
+#define KEQ_GTSV_NOALLOC_MAX_ELEMS (1 << 21)
+keq_status keq_gtsv_strided_inplace_noalloc(const double* dl, const double* d, const double* du,
+                                            double* B, int32_t n, int32_t batch,
+                                            keq_stream_t stream);
+
 
 /* K5: cuda_kernel/BGK1D1V/lo_blocktridiag/block_tridiag_binding.cpp:25-108
  * (block_tridiag_solve): batch 3x3-block tridiagonal systems of n block rows.

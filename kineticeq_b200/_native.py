@@ -105,6 +105,7 @@ _PROTOS = {
                                              _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _vp]),
     "keq_gtsv_workspace_size": (_i32, [_i32, _i32, C.POINTER(_sz)]),
     "keq_gtsv_strided_inplace": (_i32, [_dp, _dp, _dp, _dp, _i32, _i32, _vp, _sz, _vp]),
+    "keq_gtsv_strided_inplace_noalloc": (_i32, [_dp, _dp, _dp, _dp, _i32, _i32, _vp]),
     "keq_block_tridiag_workspace_size": (_i32, [_i32, _i32, C.POINTER(_sz)]),
     "keq_block_tridiag_solve": (_i32, [_dp, _dp, _dp, _dp, _dp, _i32, _i32, _vp, _sz, _vp]),
     "keq_math_selftest": (_i32, [_i32, _dp, _dp, _i32, _vp]),

@@ -32,3 +32,13 @@ struct keq_plan {
 
 // Sets plan->grid to every resident CTA of plan->kernel (occupancy query).
 keq_status keq_internal_plan_grid(keq_plan* plan);
+
+namespace keq {
+// Batched tridiagonal solve (keq_kernels.cu): one thread per system; cp is
+// n * batch doubles of scratch that every call overwrites before reading.
+__global__ void __launch_bounds__(128) gtsv_kernel(const double* __restrict__ dl,
+                                                   const double* __restrict__ d,
+                                                   const double* __restrict__ du,
+                                                   double* __restrict__ B, int n, int batch,
+                                                   double* __restrict__ cp);
+}  // namespace keq

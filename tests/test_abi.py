@@ -48,3 +48,12 @@ def test_workspace_queries_validate(lib):
     assert lib.keq_block_tridiag_workspace_size(10, 2, C.byref(nb)) == 0
     assert lib.keq_moments_n_nu_T(0, 0, 4, 4, 1.0, 0, 0, 0, 0) == 1
 
+
+
+def test_noalloc_gtsv_rejects_oversize_on_host(lib):
+    # n * batch above the fixed scratch (2^21 doubles) is refused before any
+    # CUDA call; the pointers are never dereferenced on this path
+    assert lib.keq_gtsv_strided_inplace_noalloc(8, 16, 24, 32, 2098, 1000, 0) == N.KEQ_ERR_CAPACITY
+    assert lib.keq_gtsv_strided_inplace_noalloc(8, 16, 24, 32, 1 << 21, 2, 0) == N.KEQ_ERR_CAPACITY
+    assert lib.keq_gtsv_strided_inplace_noalloc(0, 16, 24, 32, 10, 10, 0) == N.KEQ_ERR_INVALID
+    assert lib.keq_gtsv_strided_inplace_noalloc(8, 16, 24, 32, 0, 10, 0) == N.KEQ_OK
