@@ -33,6 +33,8 @@ import sys
 import time
 from pathlib import Path
 
+import numpy as np
+
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
@@ -393,13 +395,233 @@ def run_reference(args, dist, rank, world):
     print(json.dumps(out))
 
 
+# ---------------------------------------------------------------------------
+# Mixed workloads: the batching form (256 seeded uneven instances, 100 steps)
+# and the serving form (Poisson request stream with the same size and state
+# distribution, 100..2000 steps per request).
+# ---------------------------------------------------------------------------
+MIX_WORKLOADS = {
+    # name: (kind, instances, seed, rate per s)
+    "batch-cfg3-256": ("batch", 256, 0, None),
+    "serve-cfg5-r200": ("serve", 64, 0, 200.0),
+    "serve-cfg5-r50": ("serve", 32, 1, 50.0),
+}
+MIX_PARAMS = dict(picard_iter=64, picard_tol=1e-10, abs_tol=1e-16)
+
+
+def _plain_rate(descs, steps, params):
+    """Plain FP64 path: every instance alone, one launch per step."""
+    import torch
+
+    from kineticeq_b200.batch import make_state, spec_of
+    from kineticeq_b200.plan import ImplicitPlan, implicit_params_struct
+
+    t = 0.0
+    cells = 0
+    for d in descs:
+        st = make_state(d)
+        plan = ImplicitPlan([spec_of(d, st)], implicit_params_struct(None, **params))
+        plan.step(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        plan.step(steps)
+        e1.record()
+        e1.synchronize()
+        t += e0.elapsed_time(e1) / 1e3
+        cells += d.cells * steps
+    return cells / t
+
+
+def _oracle_rate(descs, params, budget_s):
+    """The oracle on the host cores over a bounded sample of the instances."""
+    from oracle import oracle as O
+
+    p = O.implicit_params(None, **params)
+    O.lib()
+    t = 0.0
+    cells = steps = 0
+    for d in descs:
+        g = O.Grid(d.nx, d.nv, d.Lx, d.v_max)
+        reg = [(r["x_range"][0], r["x_range"][1], r["n"], r["u"], r["T"]) for r in d.regions]
+        f = O.initial_condition(g, reg)
+        t0 = time.perf_counter()
+        O.implicit_step(f, g.v(), g.dx, g.dv, d.dt, d.tau_tilde, p)
+        t += time.perf_counter() - t0
+        cells += d.cells
+        steps += 1
+        if t > budget_s:
+            break
+    return cells / t, f"first time step of the first {steps} instances of the mix ({t:.1f} s)"
+
+
+def run_mix(args, dist, rank, world):
+    import torch
+
+    from kineticeq_b200 import autotune
+    from kineticeq_b200.batch import BatchSolver, sample_instances
+    from kineticeq_b200.serving import Server, plain_throughput, poisson_stream
+
+    kind, n_inst, seed, rate = MIX_WORKLOADS[args.workload]
+    table = autotune.load() or {}
+    out = {"metric": METRIC, "unit": METRIC, "n_gpus": world, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded two-state Riemann instances, sizes and states as the "
+                   "batching distribution)"}
+    launches = 0
+    if kind == "batch":
+        descs = sample_instances(n_inst, seed=seed + rank)
+        solver = BatchSolver(descs, MIX_PARAMS, table=table)
+        cells = solver.cells
+        for _ in range(args.warmup):
+            solver.step(1)
+        torch.cuda.synchronize()
+        solver.reset()
+        use_graph = args.steps % 2 == 0
+        if use_graph:
+            solver.capture(2)
+        it0 = solver.plan.stats.fetch()["total_iters"].astype(np.int64)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        _barrier(dist)
+        torch.cuda.synchronize()
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            e0.record()
+            if use_graph:
+                for _ in range(args.steps // 2):
+                    solver.replay()
+            else:
+                solver.step(args.steps)
+            e1.record()
+            torch.cuda.synchronize()
+        _barrier(dist)
+        ms = _max_over_ranks(dist, e0.elapsed_time(e1))
+        launches = args.steps
+        rec = solver.plan.stats.fetch()
+        iters = rec["total_iters"].astype(np.int64) - it0
+        cell_iters = float(sum(int(i) * d.cells for i, d in zip(iters, descs)))
+        value = world * cells * args.steps / (ms / 1e3)
+        plain = _plain_rate(descs[:64], 2, MIX_PARAMS)
+        e2e = None
+        if not args.no_e2e:
+            # per step: every instance's f^n from pinned host memory to the
+            # device, one step, f^{n+1} back to pinned host memory
+            hosts = [s.a.cpu().pin_memory() for s in solver.specs]
+            outs = [torch.empty_like(h).pin_memory() for h in hosts]
+            k2 = 2
+            solver.reset()
+            torch.cuda.synchronize()
+            q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            q0.record()
+            for _ in range(k2):
+                for i, h in enumerate(hosts):
+                    solver.plan.state(i).copy_(h, non_blocking=True)
+                solver.step(1)
+                for i, o in enumerate(outs):
+                    o.copy_(solver.plan.state(i), non_blocking=True)
+                hosts = outs
+            q1.record()
+            torch.cuda.synchronize()
+            nb = 8 * cells
+            e2e = {"value": round(world * cells * k2 / (q0.elapsed_time(q1) / 1e3), 1),
+                   "unit": METRIC, "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb}
+        out["e2e"] = e2e
+        peak, peak_kind = _peaks()
+        achieved = BYTES_PER_CELL_ITER * cell_iters / (ms / 1e3) / 1e9
+        out.update({"value": round(value, 1), "steps": args.steps, "warmup": args.warmup,
+                    "ms_per_step": round(ms / args.steps, 4),
+                    "plain_value": round(plain, 1), "speedup_vs_plain": round(value / plain, 3),
+                    "config": {"workload": args.workload, "instances": n_inst, "seed": seed,
+                               "cells_per_step": cells, "dt": 5e-6, **MIX_PARAMS,
+                               "tile_rows_table": bool(table), "cuda_graph": use_graph,
+                               "l2": "inputs larger than L2 (535 MB per FP64 field)",
+                               "mean_picard_iters_per_step":
+                                   round(cell_iters / cells / args.steps, 3),
+                               "plain": "first 64 instances, each alone, 2 steps after 1 warm-up"},
+                    "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                                 "unit": "GB/s", "frac": round(achieved / peak, 4),
+                                 "peak_kind": peak_kind, "traffic": None,
+                                 "kernel": "keq::implicit_step_kernel"},
+                    "clocks": clk.summary()})
+        sample_descs = descs
+    else:
+        reqs = poisson_stream(n_inst, rate, seed=seed + rank)
+        warm = poisson_stream(4, 1e6, seed=99, steps_range=(3, 3))
+        Server(params=MIX_PARAMS, table=table).run(warm, realtime=False)
+        _barrier(dist)
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            res = Server(params=MIX_PARAMS, table=table).run(reqs)
+        _barrier(dist)
+        ms = _max_over_ranks(dist, res["makespan_s"] * 1e3)
+        launches = res["launches"]
+        value = world * res["cell_steps"] / (ms / 1e3)
+        e2e = None
+        if not args.no_e2e:
+            # the same stream with host inputs and outputs: each request's
+            # initial state comes from pinned host memory at admission and its
+            # final state goes back to pinned host memory at retirement
+            from kineticeq_b200.batch import make_state
+
+            reqs2 = poisson_stream(n_inst, rate, seed=seed + rank)
+            for r in reqs2:
+                r.f0_host = make_state(r.desc).f.cpu().pin_memory()
+            torch.cuda.synchronize()
+            res2 = Server(params=MIX_PARAMS, table=table, copy_out=True).run(reqs2)
+            nb = sum(8 * r.desc.cells for r in reqs2)
+            e2e = {"value": round(world * res2["cell_steps"] / res2["makespan_s"], 1),
+                   "unit": METRIC, "h2d_bytes_per_step": round(nb / res2["steps"]),
+                   "d2h_bytes_per_step": round(nb / res2["steps"]),
+                   "p50_latency_s": round(res2["p50_latency_s"], 4),
+                   "p99_latency_s": round(res2["p99_latency_s"], 4)}
+        out["e2e"] = e2e
+        plain, plain_t, plain_sample = plain_throughput(reqs, MIX_PARAMS, steps_cap=10)
+        out.update({"value": round(value, 1), "steps": res["steps"], "warmup": 1,
+                    "ms_per_step": round(ms / max(res["steps"], 1), 4),
+                    "p50_latency_s": round(res["p50_latency_s"], 4),
+                    "p99_latency_s": round(res["p99_latency_s"], 4),
+                    "plain_value": round(plain, 1), "speedup_vs_plain": round(value / plain, 3),
+                    "config": {"workload": args.workload, "requests": n_inst, "rate_per_s": rate,
+                               "seed": seed, "steps_per_request": "uniform 100..2000",
+                               **MIX_PARAMS, "rebuilds": res["rebuilds"],
+                               "l2": "inputs larger than L2 in aggregate; not flushed",
+                               "plain": plain_sample},
+                    "clocks": clk.summary()})
+        sample_descs = [r.desc for r in reqs]
+    out["gpu_launches"] = launches
+    if rank == 0 and not args.no_cpu_baseline:
+        v, sample = _oracle_rate(sample_descs, MIX_PARAMS, args.cpu_seconds)
+        out["cpu_baseline"] = {"value": round(v, 1), "unit": METRIC,
+                               "cores": os.cpu_count() or 1, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def run_mix_reference(args, dist, rank, world):
+    if rank != 0:
+        return
+    from kineticeq_b200.batch import sample_instances
+
+    kind, n_inst, seed, rate = MIX_WORKLOADS[args.workload]
+    descs = sample_instances(n_inst, seed=seed,
+                             steps_range=None if kind == "batch" else (100, 2000))
+    v, sample = _oracle_rate(descs, MIX_PARAMS, args.cpu_seconds * 6)
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": METRIC,
+                      "n_gpus": world, "steps": 1, "warmup": 0, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                      "data": "synthetic", "config": {"workload": args.workload},
+                      "cpu_baseline": {"value": round(v, 1), "unit": METRIC,
+                                       "cores": os.cpu_count() or 1, "kind": "port",
+                                       "sample": sample},
+                      "e2e": {"value": round(v, 1), "unit": METRIC, "h2d_bytes_per_step": 0,
+                              "d2h_bytes_per_step": 0}}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(MIX_WORKLOADS),
+                    default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -408,10 +630,11 @@ def main():
         args.warmup = 3
     dist, rank, world = _dist()
     try:
+        mix = args.workload in MIX_WORKLOADS
         if args.impl == "reference":
-            run_reference(args, dist, rank, world)
+            (run_mix_reference if mix else run_reference)(args, dist, rank, world)
         else:
-            run_ours(args, dist, rank, world)
+            (run_mix if mix else run_ours)(args, dist, rank, world)
     finally:
         if dist is not None:
             dist.destroy_process_group()

@@ -54,6 +54,11 @@ typedef struct keq_grid {
     double dx;
     double dv;
     const double* v; /* device, nv entries, ascending */
+    /* Optional host-side facts about v that save plan creation a device read
+     * and a stream synchronisation: kp = number of velocities <= 0 and
+     * v_max = max |v|.  kp < 0 means unknown (v is then read back). */
+    int32_t kp;
+    double v_max;
 } keq_grid;
 
 /* implicit.Params: params/BGK1D1V/implicit.py:5-37 (CNN warm start excluded).
@@ -77,6 +82,14 @@ typedef struct keq_implicit_params {
     double aa_alpha_max;
     int32_t fixed_iters;
     int32_t tile_rows;
+    /* precision: 0 = FP64 (the reference's method), 1 = mixed-precision form:
+     * FP32 sweeps (Maxwellian, reciprocal and recurrence in FP32 on FP32
+     * copies of f^n and of the iterate; moments, Anderson and residuals in
+     * FP64) until a sweep meets mixed_tol (0 = 1e-6), then FP64 sweeps until
+     * picard_tol as in the FP64 form.  keq_step_stats.lo_iters reports the
+     * FP32 sweeps.  A backend knob without reference counterpart. */
+    int32_t precision;
+    double mixed_tol;
 } keq_implicit_params;
 
 /* holo.Params: params/BGK1D1V/holo.py:5-13 (+ the hidden SVdown flag read at
@@ -165,6 +178,13 @@ keq_status keq_plan_step(keq_plan* plan, int32_t n_steps, int32_t parity, keq_st
  * all warps.  No reference counterpart (profiling aid). */
 keq_status keq_plan_set_trace(keq_plan* plan, unsigned long long* trace, int32_t iters,
                               keq_stream_t stream);
+/* Implicit plans: attach a device int32 mask of n entries (or NULL to
+ * detach).  While mask[b] == 0, instance b is left untouched by every step
+ * (no state, stats or workspace write), so a serving loop can retire slots
+ * without rebuilding the plan; the mask is read on the device at every
+ * launch and may be changed by stream-ordered device writes.  Synchronises
+ * the stream.  No reference counterpart. */
+keq_status keq_plan_set_enable_mask(keq_plan* plan, const int32_t* mask, keq_stream_t stream);
 /* Device-side error bits of the plan (1 << keq_status) accumulated over every
  * launch since plan creation or the last keq_plan_reset, synchronising the
  * stream; 0 when every device-side wait completed.  A launch whose wait gave

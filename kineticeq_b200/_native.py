@@ -32,7 +32,8 @@ _sz = C.c_size_t
 
 
 class Grid(C.Structure):
-    _fields_ = [("nx", _i32), ("nv", _i32), ("dx", _f64), ("dv", _f64), ("v", _dp)]
+    _fields_ = [("nx", _i32), ("nv", _i32), ("dx", _f64), ("dv", _f64), ("v", _dp),
+                ("kp", _i32), ("v_max", _f64)]
 
 
 class ImplicitParams(C.Structure):
@@ -40,7 +41,7 @@ class ImplicitParams(C.Structure):
         ("picard_iter", _i32), ("picard_tol", _f64), ("abs_tol", _f64), ("conv_type", _i32),
         ("aa_enable", _i32), ("aa_m", _i32), ("aa_beta", _f64), ("aa_stride", _i32),
         ("aa_start_iter", _i32), ("aa_reg", _f64), ("aa_alpha_max", _f64),
-        ("fixed_iters", _i32), ("tile_rows", _i32),
+        ("fixed_iters", _i32), ("tile_rows", _i32), ("precision", _i32), ("mixed_tol", _f64),
     ]
 
 
@@ -87,6 +88,7 @@ _PROTOS = {
     "keq_plan_step": (_i32, [_vp, _i32, _i32, _vp]),
     "keq_plan_error": (_i32, [_vp, _vp, C.POINTER(_i32)]),
     "keq_plan_reset": (_i32, [_vp, _vp]),
+    "keq_plan_set_enable_mask": (_i32, [_vp, _dp, _vp]),
     "keq_plan_set_spin_limit": (_i32, [_vp, C.c_uint64, _vp]),
     "keq_plan_set_trace": (_i32, [_vp, _vp, _i32, _vp]),
     "keq_plan_destroy": (None, [_vp]),

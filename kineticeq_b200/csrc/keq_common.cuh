@@ -209,7 +209,7 @@ struct PlanHead {
     unsigned long long seq;     // launch sequence (epochs of look-back flags)
     unsigned long long* trace;  // optional phase trace (profiling aid)
     int trace_iters;
-    int pad;
+    int fresh;                  // 1 until the first launch completes: stats totals start at 0
 };
 
 // Spin (bounded) until *flag >= want.  Returns false on timeout.

@@ -401,12 +401,22 @@ __device__ __noinline__ double lo_prep_row(const HoloInst& I, int k) {
         Q3[t] = q_of(m3[t]);
     }
     // face moments S(f) of faces f = i-1 (L) and i (R) (_HO_calculate_moments_face):
-    // upwind state: v > 0 from the left cell, v <= 0 from the right cell
+    // upwind state: v > 0 from the left cell, v <= 0 from the right cell.
+    // With the consistency terms off the reference keeps the face moments of
+    // the step's f^n (:459-462); with them on, _compute_Y_I_terms replaces
+    // them by those of f_z (:163-165).
+    double Rs[3][8];
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        const double* src = (I.con_terms ? I.R : I.Rn) + 8 * (size_t)(i - 1 + t);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) Rs[t][q] = I.con_terms ? Rr[t][q] : __ldcg(&src[q]);
+    }
     double S[2][3];
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
-        const double* Lr = Rr[s];
-        const double* Rg = Rr[s + 1];
+        const double* Lr = Rs[s];
+        const double* Rg = Rs[s + 1];
         if (I.sv_down) {
             S[s][0] = (Lr[0] + Rg[4]) * dv;
             S[s][1] = (Lr[1] + Rg[5]) * dv;
@@ -1030,7 +1040,15 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
         const HoloInst& I = P.inst[b];
         const double* fn = swap_io ? I.f_out : I.f_in;
         double* fo = swap_io ? const_cast<double*>(I.f_in) : I.f_out;
-        if (threadIdx.x == 0) I.stats->status = KEQ_ERR_TIMEOUT;  // pending until stage E
+        if (threadIdx.x == 0) {
+            I.stats->status = KEQ_ERR_TIMEOUT;  // pending until stage E
+            if (P.head.fresh) {
+                I.stats->total_iters = 0;
+                I.stats->total_steps = 0;
+            }
+        }
+        const long long ntiles = (long long)I.nvt * I.nchunks;
+        for (long long q = threadIdx.x; q < ntiles; q += kThreads) I.flag[q] = 0ull;
         for (int q = threadIdx.x; q < 4 * I.ho_iter; q += kThreads) I.ho_red[q] = 0.0;
         for (int q = threadIdx.x; q < 2 * I.ho_iter * I.lo_iter; q += kThreads) I.lo_hist[q] = 0.0;
         for (int q = threadIdx.x; q < I.ho_iter * I.lo_iter; q += kThreads) I.lo_run[q] = 0;
@@ -1242,6 +1260,7 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
     }
 
     // E: statistics (benchlog keys of :586-594)
+    if (blockIdx.x == 0 && threadIdx.x == 0) P.head.fresh = 0;
     for (int b = blockIdx.x; b < n_inst; b += G) {
         if (threadIdx.x != 0) continue;
         const HoloInst& I = P.inst[b];
@@ -1485,21 +1504,24 @@ keq_status keq_holo_plan_create(const keq_instance* insts, int32_t n, const keq_
             delete plan;
             return KEQ_ERR_WORKSPACE;
         }
-        vh.resize(nv);
-        if (cudaMemcpyAsync(vh.data(), in.grid.v, sizeof(double) * nv, cudaMemcpyDeviceToHost, s) !=
-                cudaSuccess ||
-            cudaStreamSynchronize(s) != cudaSuccess) {
-            keq_internal_set_cuda_error(cudaGetLastError());
-            delete plan;
-            return KEQ_ERR_CUDA;
-        }
-        int kp = 0;
-        for (int j = 0; j < nv; ++j) {
-            if (j > 0 && !(vh[j] > vh[j - 1])) {
+        int kp = in.grid.kp;
+        if (kp < 0 || kp > nv) {
+            vh.resize(nv);
+            if (cudaMemcpyAsync(vh.data(), in.grid.v, sizeof(double) * nv, cudaMemcpyDeviceToHost,
+                                s) != cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess) {
+                keq_internal_set_cuda_error(cudaGetLastError());
                 delete plan;
-                return KEQ_ERR_INVALID;
+                return KEQ_ERR_CUDA;
             }
-            if (!(vh[j] > 0.0)) kp = j + 1;
+            kp = 0;
+            for (int j = 0; j < nv; ++j) {
+                if (j > 0 && !(vh[j] > vh[j - 1])) {
+                    delete plan;
+                    return KEQ_ERR_INVALID;
+                }
+                if (!(vh[j] > 0.0)) kp = j + 1;
+            }
         }
         const HDerived d = hderive(nx, nv, kp);
         if (d.lo_len > holo::kMaxLoChunk || d.lo_k > holo::kMaxLoChunks) {
@@ -1520,8 +1542,6 @@ keq_status keq_holo_plan_create(const keq_instance* insts, int32_t n, const keq_
         I.lo_abs_tol = p.lo_abs_tol;
         I.v = in.grid.v; I.f_in = in.f_in; I.f_out = in.f_out; I.stats = in.stats;
         carve_holo(in.workspace, nx, nv, kp, p, &I);
-        e = cudaMemsetAsync(I.flag, 0, sizeof(unsigned long long) * (size_t)d.nvt * d.nchunks, s);
-        if (e != cudaSuccess) break;
         host[b] = I;
         toff[b] = t; roff[b] = r; loff[b] = l;
         t += (long long)d.nvt * d.nchunks;
@@ -1548,6 +1568,7 @@ keq_status keq_holo_plan_create(const keq_instance* insts, int32_t n, const keq_
     unsigned* tickets = c.take<unsigned>(max_ho + 1);
     HoloDev h{};
     h.head.spin_limit = kSpinLimit;
+    h.head.fresh = 1;  // the first launch zeroes the stats totals
     h.n_inst = n;
     h.max_ho = max_ho;
     h.max_lo = max_lo;
@@ -1570,10 +1591,6 @@ keq_status keq_holo_plan_create(const keq_instance* insts, int32_t n, const keq_
         e = cudaMemcpyAsync(dr_, roff.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(dl_, loff.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess)
-        for (int b = 0; b < n && e == cudaSuccess; ++b)
-            e = cudaMemsetAsync(insts[b].stats, 0, sizeof(keq_step_stats), s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         keq_internal_set_cuda_error(e);
         delete plan;

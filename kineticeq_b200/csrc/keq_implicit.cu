@@ -67,10 +67,13 @@ struct ImpInst {
     double tol, abs_tol;
     int aa_on, aa_cols, aa_stride, aa_start;
     double aa_beta, aa_reg, aa_alpha_max;
+    int mixed, pad2;  // mixed-precision form: FP32 sweeps, then FP64 sweeps
+    double tol32;     // Picard tolerance that ends the FP32 sweeps
     const double* v;
     const double* f_in;
     double* f_out;
     keq_step_stats* stats;
+    const int* enable;  // optional device flag: 0 = leave this instance untouched this step
     // workspace carve
     double* W;       // 3*nx  : n | nu | T   (W^(m))
     double* Wn;      // 3*nx  : moments of the newest iterate (unfloored)
@@ -89,6 +92,8 @@ struct ImpInst {
     double* gpart;   // nrb * kMaxPairs
     double* alpha;   // picard_iter * kMaxAACols
     unsigned* rbdone;// picard_iter
+    float* fn32;     // nx*nv (mixed form): f^n in FP32, written by P1
+    float* x32;      // nx*nv (mixed form): the FP32 iterate, updated in place
 };
 
 // Device header of an implicit plan (starts with the common PlanHead).
@@ -115,16 +120,33 @@ struct WarpSmem {
     int done_rb[2];
 };
 
+// Mixed-precision form: iteration m is an FP32 sweep while no earlier sweep
+// met the FP32-phase tolerance tol32 (all earlier iterations are then FP32
+// sweeps too) and m is in the first half of the iteration cap; every later
+// iteration is an FP64 sweep with the reference's tolerance.  Replays
+// (fixed_iters) run in FP64 only.
+__device__ __forceinline__ bool fp32_iter(const ImpInst& I, int m) {
+    if (!I.mixed || I.fixed_iters > 0 || m >= I.picard_iter / 2) return false;
+    for (int k = 0; k < m; ++k)
+        if (ld_cg(&I.res[2 * k]) <= 1.0) return false;
+    return true;
+}
+
 __device__ __forceinline__ bool iter_done(const ImpInst& I, int m) {
     // Convergence test of iteration m (bgk1d_implicit_cuda_kernel.py:241).
     if (I.fixed_iters > 0) return m + 1 >= I.fixed_iters;
+    if (fp32_iter(I, m)) return false;  // an FP32 sweep never ends the step
     const double r = ld_cg(&I.res[2 * m]);
     return r <= 1.0;
 }
 
+__device__ __forceinline__ bool inst_enabled(const ImpInst& I) {
+    return I.enable == nullptr || __ldcg(I.enable) != 0;
+}
+
 __device__ __forceinline__ bool inst_active(const ImpInst& I, int m) {
     if (m >= I.picard_iter) return false;
-    if (m == 0) return true;
+    if (m == 0) return inst_enabled(I);
     if (__ldcg(&I.st[m - 1]) != 1) return false;
     return !iter_done(I, m - 1);
 }
@@ -248,6 +270,9 @@ __device__ void moments_tile(WarpSmem& w, int vt, int c, const double* __restric
     cp_async_wait_all();
     if (!g.lane_ok)
         for (int r = 0; r < g.nrows; ++r) w.a[r][lane] = 0.0;
+    else if (I.mixed)
+        for (int r = 0; r < g.nrows; ++r)
+            I.fn32[(size_t)scan_row(I.nx, g.pos, g.s0 + r) * I.nv + g.j] = (float)w.a[r][lane];
     store_partials(w, g, vt);
 }
 
@@ -325,10 +350,15 @@ __device__ bool picard_tile(WarpSmem& w, int vt, int c, int m, unsigned long lon
     const TileGeo g = inst_tile(I, vt, c, lane);
     const int nx = I.nx, nv = I.nv;
     const int nr = g.nrows;
-    // f^n rows and the residual reference f^(m) (f^n itself at m = 0)
+    // f^n rows and the residual reference f^(m) (f^n itself at m = 0; the
+    // FP32 iterate after the FP32 sweeps of the mixed form)
+    const bool ref32 = m > 0 && fp32_iter(I, m - 1);
     stage_rows<33>(w.a, fn, g, nx, nv);
-    stage_rows<32>(w.o, m > 0 ? fo : fn, g, nx, nv);
+    if (!ref32) stage_rows<32>(w.o, m > 0 ? fo : fn, g, nx, nv);
     cp_async_commit();
+    if (ref32 && g.lane_ok)
+        for (int r = 0; r < nr; ++r)
+            w.o[r][lane] = (double)__ldcg(&I.x32[(size_t)scan_row(nx, g.pos, g.s0 + r) * nv + g.j]);
     const double vj = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
     w.vv[lane] = vj;
     stage_coeffs(w, g, vt, m);
@@ -381,7 +411,6 @@ __device__ bool picard_tile(WarpSmem& w, int vt, int c, int m, unsigned long lon
         const double x = g.lane_ok ? X : 0.0;
         w.a[r][lane] = x;
         if (g.lane_ok) {
-            fo[(size_t)scan_row(nx, g.pos, g.s0 + r) * nv + g.j] = x;
             const double o = w.o[r][lane];
             const double df = fabs(x - o);
             const double ref = nan_max(fabs(x), fabs(o));
@@ -392,6 +421,115 @@ __device__ bool picard_tile(WarpSmem& w, int vt, int c, int m, unsigned long lon
     }
     store_partials(w, g, vt);
     return ok;
+}
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+// FP32 sweep of the mixed-precision form over one tile: the same assembly,
+// look-back and recurrence with the Maxwellian, the reciprocal and the
+// recurrence in FP32 on the FP32 copies of f^n and of the iterate (12 bytes
+// per cell instead of 24); the residual (against tol32) and the partial
+// moments are accumulated in FP64.
+__device__ bool picard_tile32(WarpSmem& w, int vt, int c, int m, unsigned long long epoch,
+                              unsigned long long limit, const double* __restrict__ fn,
+                              FracMax& q1, FracMax& q2, bool& bad) {
+    const ImpInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const TileGeo g = inst_tile(I, vt, c, lane);
+    const int nx = I.nx, nv = I.nv;
+    const int nr = g.nrows;
+    float(*fa)[32] = reinterpret_cast<float(*)[32]>(&w.o[0][0]);  // f^n (FP32)
+    float(*fb)[32] = fa + kRmax;                                   // previous iterate
+    const float* ref = m > 0 ? I.x32 : I.fn32;
+    if (g.lane_ok) {
+#pragma unroll 8
+        for (int r = 0; r < nr; ++r) {
+            const size_t off = (size_t)scan_row(nx, g.pos, g.s0 + r) * nv + g.j;
+            cp_async4(&fa[r][lane], I.fn32 + off);
+            cp_async4(&fb[r][lane], ref + off);
+        }
+    }
+    cp_async_commit();
+    const double vjd = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
+    w.vv[lane] = vjd;
+    stage_coeffs(w, g, vt, m);
+    cp_async_wait_all();
+    __syncwarp();
+    const float vj = (float)vjd;
+    const float cpl = (float)(I.dtdx * fabs(vjd));
+    const float one_plus = 1.0f + cpl;
+    float P = 1.0f, Y = 0.0f;
+    float cvs[kRmax];
+#pragma unroll
+    for (int r = 0; r < kRmax; ++r) {
+        cvs[r] = 0.0f;
+        if (r < nr) {
+            const float diff = vj - (float)w.coef[r][0];
+            const float dti = (float)w.coef[r][3];
+            const float M = (float)w.coef[r][2] * expf(diff * diff * (float)w.coef[r][1]);
+            const float rr = 1.0f / (one_plus + dti);
+            const float fnv = g.lane_ok ? fa[r][lane] : 0.0f;
+            const float cv = fmaf(dti, M, fnv) * rr;
+            const float av = cpl * rr;
+            cvs[r] = cv;
+            Y = fmaf(av, Y, cv);
+            P = P * av;
+        }
+    }
+    const size_t tid = (size_t)c * I.nvt + vt;
+    bool ok = true;
+    double Xd;
+    if (c == 0) {
+        Xd = g.lane_ok ? (double)__ldg(&fn[(size_t)(g.pos ? 0 : nx - 1) * nv + g.j]) : 0.0;
+    } else {
+        publish_agg(I.agg, I.flag, tid, (double)P, (double)Y, epoch);
+        ok = lookback(I.agg, I.inc, I.flag, I.nvt, vt, c, epoch, limit, Xd);
+    }
+    if (c + 1 < I.nchunks) publish_inc(I.inc, I.flag, tid, fma((double)P, Xd, (double)Y), epoch);
+    float X = (float)Xd;
+    const double tol = I.tol32, abs_tol = I.abs_tol;
+#pragma unroll
+    for (int r = 0; r < kRmax; ++r) {
+        if (r < nr) {
+            const float a = cpl / (one_plus + (float)w.coef[r][3]);
+            X = fmaf(a, X, cvs[r]);
+            const float x = g.lane_ok ? X : 0.0f;
+            w.a[r][lane] = (double)x;
+            if (g.lane_ok) {
+                const double o = (double)fb[r][lane];
+                const double df = fabs((double)x - o);
+                const double rf = nan_max(fabs((double)x), fabs(o));
+                q1.add(df, abs_tol + tol * rf);
+                q2.add(df, (rf != rf || rf >= abs_tol) ? rf : abs_tol);
+                bad |= !isfinite(x);
+            }
+        }
+    }
+    store_partials(w, g, vt);
+    return ok;
+}
+
+// Write the tile's new iterate (held in w.a) to HBM: FP64 into fo, or FP32
+// into the mixed form's iterate.  Done after the row-block arrival, so the
+// fence of that arrival does not wait for these stores.
+__device__ __forceinline__ void write_tile(WarpSmem& w, int vt, int c, double* __restrict__ fo,
+                                           bool fp32) {
+    const ImpInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const TileGeo g = inst_tile(I, vt, c, lane);
+    if (!g.lane_ok) return;
+    if (fp32) {
+#pragma unroll 8
+        for (int r = 0; r < g.nrows; ++r)
+            I.x32[(size_t)scan_row(I.nx, g.pos, g.s0 + r) * I.nv + g.j] = (float)w.a[r][lane];
+    } else {
+#pragma unroll 8
+        for (int r = 0; r < g.nrows; ++r)
+            fo[(size_t)scan_row(I.nx, g.pos, g.s0 + r) * I.nv + g.j] = w.a[r][lane];
+    }
 }
 
 // ---- Anderson: small symmetric solve (Cholesky, min-norm fall-back) -------
@@ -482,12 +620,30 @@ __device__ __noinline__ void aa_finalize(const double* gpart, int nrb, int mh, d
                                          double alpha_max, double* alpha_out) {
     const int lane = threadIdx.x & 31;
     double A[kMaxAACols * kMaxAACols];
+    // every pair's sum over the row blocks: lane L takes blocks L, L+32, ...
+    // with all pairs of a block loaded at once, then a fixed butterfly
+    const int npairs = mh * (mh + 1) / 2;
+    double acc[kMaxPairs];
+#pragma unroll
+    for (int q = 0; q < kMaxPairs; ++q) acc[q] = 0.0;
+    for (int r2 = lane; r2 < nrb; r2 += 32) {
+        const double* gp = gpart + (size_t)r2 * kMaxPairs;
+        double t[kMaxPairs];
+#pragma unroll
+        for (int q = 0; q < kMaxPairs; ++q) t[q] = q < npairs ? ld_cg(&gp[q]) : 0.0;
+#pragma unroll
+        for (int q = 0; q < kMaxPairs; ++q) acc[q] += t[q];
+    }
+#pragma unroll
+    for (int q = 0; q < kMaxPairs; ++q)
+        if (q < npairs) acc[q] = warp_sum(acc[q]);
     int pj = 0;
     for (int p = 0; p < mh; ++p)
         for (int q = p; q < mh; ++q, ++pj) {
-            double part_sum = 0.0;
-            for (int r2 = lane; r2 < nrb; r2 += 32) part_sum += ld_cg(&gpart[(size_t)r2 * kMaxPairs + pj]);
-            const double sv = warp_sum(part_sum);
+            double sv = 0.0;
+#pragma unroll
+            for (int u = 0; u < kMaxPairs; ++u)
+                if (u == pj) sv = acc[u];
             A[p * mh + q] = sv;
             A[q * mh + p] = sv;
         }
@@ -731,11 +887,21 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
     }
     for (int b = blockIdx.x; b < n_inst; b += G) {
         const ImpInst& I = P.inst[b];
+        if (!inst_enabled(I)) continue;
         const double* fn = swap_io ? I.f_out : I.f_in;
         double* fo = swap_io ? const_cast<double*>(I.f_in) : I.f_out;
         // pending status: stays KEQ_ERR_TIMEOUT unless stage E of this launch
         // runs, i.e. when a device-side wait gave up and the CTAs returned
-        if (threadIdx.x == 0) I.stats->status = KEQ_ERR_TIMEOUT;
+        if (threadIdx.x == 0) {
+            I.stats->status = KEQ_ERR_TIMEOUT;
+            if (P.head.fresh) {
+                I.stats->total_iters = 0;
+                I.stats->total_steps = 0;
+            }
+        }
+        // look-back flags: epoch 0 is never current
+        const long long ntiles = (long long)I.nvt * I.nchunks;
+        for (long long q = threadIdx.x; q < ntiles; q += kThreads) I.flag[q] = 0ull;
         for (int q = threadIdx.x; q < 2 * I.picard_iter; q += kThreads) I.res[q] = 0.0;
         for (int q = threadIdx.x; q < I.picard_iter; q += kThreads) {
             I.st[q] = 0;
@@ -772,6 +938,7 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
     for (long long t = gwarp; t < total_tiles; t += nwarps) {
         const int b = find_inst(P.tile_off, n_inst, t);
         stage_warp(w, &P.inst[b], b);
+        if (!inst_enabled(w.I)) continue;
         const long long tl = t - w.I.tile_off;
         const int c = (int)(tl / w.I.nvt), vt = (int)(tl % w.I.nvt);
         moments_tile(w, vt, c, swap_io ? w.I.f_out : w.I.f_in);
@@ -782,6 +949,7 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
     for (long long u = gwarp; u < total_rb; u += nwarps) {
         const int b = find_inst(P.rb_off, n_inst, u);
         stage_warp(w, &P.inst[b], b);
+        if (!inst_enabled(w.I)) continue;
         init_block(w, (int)(u - w.I.rb_off));
     }
     if (!plan_sync(P, G)) return;
@@ -809,7 +977,10 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
             const int c = (int)(tl / w.I.nvt), vt = (int)(tl % w.I.nvt);
             const double* fn = swap_io ? w.I.f_out : w.I.f_in;
             double* fo = swap_io ? const_cast<double*>(w.I.f_in) : w.I.f_out;
-            if (!picard_tile(w, vt, c, m, epoch, limit, fn, fo, q1, q2, bad)) {
+            const bool is32 = fp32_iter(w.I, m);
+            const bool ok = is32 ? picard_tile32(w, vt, c, m, epoch, limit, fn, q1, q2, bad)
+                                 : picard_tile(w, vt, c, m, epoch, limit, fn, fo, q1, q2, bad);
+            if (!ok) {
                 if (lane == 0) {
                     atomicOr(&P.head.err, 1 << KEQ_ERR_TIMEOUT);
                     atomicOr(&P.head.err_sticky, 1 << KEQ_ERR_TIMEOUT);
@@ -823,6 +994,7 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
                 rowblock_arrive(w.I.rbcnt + (size_t)m * w.I.nrb, w.I.nx, w.I.n_inner, w.I.nvt, g,
                                 w.done_rb);
             __syncwarp();
+            write_tile(w, vt, c, fo, is32);
             const int d0 = w.done_rb[0], d1 = w.done_rb[1];
             if (d0 >= 0 || d1 >= 0) {
                 fence_acq_rel();
@@ -837,9 +1009,11 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
     }
 
     // E: statistics
+    if (blockIdx.x == 0 && threadIdx.x == 0) P.head.fresh = 0;
     for (int b = blockIdx.x; b < n_inst; b += G) {
         if (threadIdx.x != 0) continue;
         const ImpInst& I = P.inst[b];
+        if (!inst_enabled(I)) continue;
         int last = -1;
         for (int m = 0; m < I.picard_iter; ++m) {
             if (__ldcg(&I.st[m]) == 1) last = m;
@@ -855,7 +1029,9 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
         s->status = status;
         s->iters = last + 1;
         s->aa_applied = aa_applied;
-        s->lo_iters = 0;
+        int n32 = 0;
+        while (n32 <= last && fp32_iter(I, n32)) ++n32;
+        s->lo_iters = n32;  // implicit: FP32 sweeps of the mixed-precision form
         s->residual = last >= 0 ? ld_cg(&I.res[2 * last + 1]) : 0.0;
         s->std_residual = last >= 0 ? ld_cg(&I.res[2 * last]) : 0.0;
         s->lo_residual = 0.0;
@@ -941,11 +1117,16 @@ size_t carve_instance(void* base, int nx, int nv, int kp, const keq_implicit_par
     double* gpart = c.take<double>(d.aa_on ? (size_t)d.nrb * keq::kMaxPairs : 1);
     double* alpha = c.take<double>((size_t)it * keq::kMaxAACols);
     unsigned* rbdone = c.take<unsigned>(it);
+    const bool mixed = p.precision == 1;
+    float* fn32 = c.take<float>(mixed ? (size_t)nx * nv : 1);
+    float* x32 = c.take<float>(mixed ? (size_t)nx * nv : 1);
     if (I) {
         I->W = W; I->Wn = Wn; I->Wc = Wc; I->Wb = Wb; I->part = part; I->agg = agg;
         I->inc = inc; I->flag = flag; I->rbcnt = rbcnt; I->res = res; I->st = st;
         I->nonfin = nonfin; I->aaG = aaG; I->aaR = aaR; I->gpart = gpart; I->alpha = alpha;
         I->rbdone = rbdone;
+        I->fn32 = fn32;
+        I->x32 = x32;
     }
     return align_up(c.off, 256);
 }
@@ -957,6 +1138,8 @@ bool valid_params(const keq_implicit_params& p) {
     if (p.tile_rows != 0 && p.tile_rows != 8 && p.tile_rows != 16 && p.tile_rows != 24 &&
         p.tile_rows != 32)
         return false;
+    if (p.precision != 0 && p.precision != 1) return false;
+    if (p.precision == 1 && !(p.mixed_tol >= 0.0)) return false;
     return true;
 }
 
@@ -1082,23 +1265,27 @@ keq_status keq_implicit_plan_create(const keq_instance* insts, int32_t n,
             delete plan;
             return KEQ_ERR_WORKSPACE;
         }
-        vh.resize(nv);
-        if (cudaMemcpyAsync(vh.data(), in.grid.v, sizeof(double) * nv, cudaMemcpyDeviceToHost, s) !=
-                cudaSuccess ||
-            cudaStreamSynchronize(s) != cudaSuccess) {
-            keq_internal_set_cuda_error(cudaGetLastError());
-            delete plan;
-            return KEQ_ERR_CUDA;
-        }
-        int kp = 0;
-        double vmax = 0.0;
-        for (int j = 0; j < nv; ++j) {
-            if (j > 0 && !(vh[j] > vh[j - 1])) {
+        int kp = in.grid.kp;
+        double vmax = in.grid.v_max;
+        if (kp < 0 || kp > nv || !(vmax > 0.0)) {
+            vh.resize(nv);
+            if (cudaMemcpyAsync(vh.data(), in.grid.v, sizeof(double) * nv, cudaMemcpyDeviceToHost,
+                                s) != cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess) {
+                keq_internal_set_cuda_error(cudaGetLastError());
                 delete plan;
-                return KEQ_ERR_INVALID;  // v must be strictly ascending
+                return KEQ_ERR_CUDA;
             }
-            if (!(vh[j] > 0.0)) kp = j + 1;
-            vmax = fmax(vmax, fabs(vh[j]));
+            kp = 0;
+            vmax = 0.0;
+            for (int j = 0; j < nv; ++j) {
+                if (j > 0 && !(vh[j] > vh[j - 1])) {
+                    delete plan;
+                    return KEQ_ERR_INVALID;  // v must be strictly ascending
+                }
+                if (!(vh[j] > 0.0)) kp = j + 1;
+                vmax = fmax(vmax, fabs(vh[j]));
+            }
         }
         const Derived d = derive(nx, nv, kp, p);
         ImpInst I{};
@@ -1114,16 +1301,11 @@ keq_status keq_implicit_plan_create(const keq_instance* insts, int32_t n,
         I.aa_on = d.aa_on; I.aa_cols = d.aa_cols; I.aa_stride = p.aa_stride;
         I.aa_start = p.aa_start_iter; I.aa_beta = p.aa_beta; I.aa_reg = p.aa_reg;
         I.aa_alpha_max = p.aa_alpha_max;
+        I.mixed = p.precision == 1 ? 1 : 0;
+        I.tol32 = p.mixed_tol > 0.0 ? p.mixed_tol : 1e-6;
+        if (I.tol32 < p.picard_tol) I.tol32 = p.picard_tol;
         I.v = in.grid.v; I.f_in = in.f_in; I.f_out = in.f_out; I.stats = in.stats;
         carve_instance(in.workspace, nx, nv, kp, p, &I);
-        // look-back flags start at epoch 0 (never current): a workspace that
-        // held another plan cannot leave flags that look published
-        e = cudaMemsetAsync(I.flag, 0, sizeof(unsigned long long) * (size_t)d.nvt * d.nchunks, s);
-        if (e != cudaSuccess) {
-            keq_internal_set_cuda_error(e);
-            delete plan;
-            return KEQ_ERR_CUDA;
-        }
         host_inst[b] = I;
         tile_off[b] = toff;
         rb_off[b] = roff;
@@ -1146,6 +1328,7 @@ keq_status keq_implicit_plan_create(const keq_instance* insts, int32_t n,
     unsigned* tickets = c.take<unsigned>(max_iter + 1);
     PlanDev h{};
     h.head.spin_limit = kSpinLimit;
+    h.head.fresh = 1;  // the first launch zeroes the stats totals
     h.head.seq = 0ull;
     h.n_inst = n;
     h.max_iter = max_iter;
@@ -1167,11 +1350,6 @@ keq_status keq_implicit_plan_create(const keq_instance* insts, int32_t n,
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(droff, rb_off.data(), sizeof(long long) * (n + 1),
                             cudaMemcpyHostToDevice, s);
-    // stats start from zero totals
-    if (e == cudaSuccess)
-        for (int b = 0; b < n && e == cudaSuccess; ++b)
-            e = cudaMemsetAsync(insts[b].stats, 0, sizeof(keq_step_stats), s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // host staging must outlive the copies
     if (e != cudaSuccess) {
         keq_internal_set_cuda_error(e);
         delete plan;
@@ -1183,6 +1361,23 @@ keq_status keq_implicit_plan_create(const keq_instance* insts, int32_t n,
         return gs;
     }
     *plan_out = plan;
+    return KEQ_OK;
+}
+
+keq_status keq_plan_set_enable_mask(keq_plan* plan, const int32_t* mask, keq_stream_t stream) {
+    if (!plan || plan->kind != KEQ_PLAN_IMPLICIT) return KEQ_ERR_INVALID;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    for (int b = 0; b < plan->n_inst; ++b) {
+        ImpInst* rec = reinterpret_cast<ImpInst*>(plan->host_inst.data()) + b;
+        rec->enable = mask ? mask + b : nullptr;
+    }
+    cudaError_t e = cudaMemcpyAsync(plan->dev_inst, plan->host_inst.data(),
+                                    sizeof(ImpInst) * plan->n_inst, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        keq_internal_set_cuda_error(e);
+        return KEQ_ERR_CUDA;
+    }
     return KEQ_OK;
 }
 

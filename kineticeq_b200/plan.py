@@ -28,10 +28,15 @@ assert _STATS_DTYPE.itemsize == N.STATS_BYTES
 
 
 def implicit_params_struct(sp=None, fixed_iters: int = 0, tile_rows: int = 0,
+                           precision: str = "fp64", mixed_tol: float = 0.0,
                            **kw) -> N.ImplicitParams:
     """implicit.Params (or keywords) -> keq_implicit_params; the clamps of
     bgk1d_implicit_cuda_kernel.py:49-65 are applied inside the library.
-    tile_rows (8/16/24/32, 0 = default) is this backend's tile height."""
+    tile_rows (8/16/24/32, 0 = default) is this backend's tile height;
+    precision "fp64" (the reference's method) or "mixed" (FP32 sweeps, then
+    FP64 sweeps to picard_tol)."""
+    if precision not in ("fp64", "mixed"):
+        raise ValueError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
     g = (lambda k, d: kw[k] if k in kw else getattr(sp, k, d))
     conv = str(g("conv_type", "f")).lower()
     if conv not in ("f", "w"):
@@ -41,13 +46,15 @@ def implicit_params_struct(sp=None, fixed_iters: int = 0, tile_rows: int = 0,
         1 if conv == "w" else 0, int(bool(g("aa_enable", False))), int(g("aa_m", 6)),
         float(g("aa_beta", 1.0)), int(g("aa_stride", 1)), int(g("aa_start_iter", 2)),
         float(g("aa_reg", 1e-10)), float(g("aa_alpha_max", 50.0)), int(fixed_iters),
-        int(tile_rows))
+        int(tile_rows), 1 if precision == "mixed" else 0, float(mixed_tol))
 
 
 @dataclass
 class InstanceSpec:
     """One solve: grid (nx, nv, dx, dv, v on the device), dt, tau_tilde and
-    the two (nx, nv) FP64 device buffers; ``a`` holds f^n on entry."""
+    the two (nx, nv) FP64 device buffers; ``a`` holds f^n on entry.  ``kp``
+    (number of velocities <= 0) and ``v_max`` (max |v|) may be given when the
+    host knows v, which spares plan creation a device read."""
     v: torch.Tensor
     dx: float
     dv: float
@@ -55,6 +62,8 @@ class InstanceSpec:
     tau_tilde: float
     a: torch.Tensor
     b: torch.Tensor
+    kp: int = -1
+    v_max: float = 0.0
 
     @property
     def nx(self) -> int:
@@ -192,7 +201,8 @@ class _StepPlan:
             if s.a.shape != s.b.shape or s.a.dim() != 2 or s.v.numel() != s.a.shape[1]:
                 raise RuntimeError("f / f_tmp must be (nx, nv) and v must be (nv,)")
             p = pstructs[i if len(pstructs) > 1 else 0]
-            grid = N.Grid(s.nx, s.nv, float(s.dx), float(s.dv), s.v.data_ptr())
+            grid = N.Grid(s.nx, s.nv, float(s.dx), float(s.dv), s.v.data_ptr(), int(s.kp),
+                          float(s.v_max))
             nbytes = C.c_size_t(0)
             N.check(self._ws_query(lib, grid, p, nbytes), "workspace query")
             ws = torch.empty((max(int(nbytes.value), 256),), dtype=torch.uint8,
@@ -225,6 +235,13 @@ class _StepPlan:
         if self._ring is None:
             self._ring = StatsRing(self.stats_dev, self.n)
         return self._ring.capture(self._stream)
+
+    def set_enable_mask(self, mask) -> None:
+        """Attach a device int32 mask (one entry per instance; 0 = skip) or None."""
+        ptr = 0 if mask is None else mask.data_ptr()
+        N.check(self._lib.keq_plan_set_enable_mask(self._h, ptr, N.stream_handle(self._stream)),
+                "enable mask")
+        self._mask = mask
 
     def reset_errors(self) -> None:
         """Clear the accumulated device error bits (keq_plan_reset)."""
@@ -337,6 +354,14 @@ def grid_of(nx: int, nv: int, Lx: float = 1.0, v_max: float = 10.0, device="cuda
     """(v on device, dx, dv) exactly as core/states/state_1d.py:30-58."""
     v = torch.linspace(-v_max, v_max, nv, dtype=torch.float64).to(device)
     return v, float(Lx / (nx - 1)), float((2.0 * v_max) / (nv - 1))
+
+
+def velocity_facts(nv: int, v_max: float = 10.0):
+    """(kp, max |v|) of the velocity grid linspace(-v_max, v_max, nv), computed
+    on the host from the same float64 linspace."""
+    vh = torch.linspace(-v_max, v_max, nv, dtype=torch.float64)
+    kp = int((vh <= 0.0).sum())
+    return kp, float(vh.abs().max())
 
 
 def _inv_sqrt_2pi() -> float:

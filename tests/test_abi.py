@@ -31,12 +31,12 @@ def test_status_strings(lib):
 
 
 def test_workspace_queries_validate(lib):
-    g = N.Grid(256, 128, 1 / 255, 20 / 127, 0)
-    p = N.ImplicitParams(64, 1e-10, 1e-16, 0, 0, 5, 1.0, 1, 2, 1e-10, 50.0, 0, 0)
+    g = N.Grid(256, 128, 1 / 255, 20 / 127, 0, -1, 0.0)
+    p = N.ImplicitParams(64, 1e-10, 1e-16, 0, 0, 5, 1.0, 1, 2, 1e-10, 50.0, 0, 0, 0, 0.0)
     nb = C.c_size_t(0)
     assert lib.keq_implicit_instance_workspace_size(C.byref(g), C.byref(p), C.byref(nb)) == 0
     assert nb.value > 256 * 4 * 8
-    bad = N.Grid(2, 128, 1.0, 1.0, 0)
+    bad = N.Grid(2, 128, 1.0, 1.0, 0, -1, 0.0)
     assert lib.keq_implicit_instance_workspace_size(C.byref(bad), C.byref(p), C.byref(nb)) == 1
     p.picard_iter = 0
     assert lib.keq_implicit_instance_workspace_size(C.byref(g), C.byref(p), C.byref(nb)) == 1
