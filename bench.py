@@ -93,11 +93,14 @@ def _peaks():
 
 
 def _traffic_from_profiles(workload: str):
-    """Per-launch DRAM bytes recorded by the committed ncu summary, scaled to
-    this workload (profiles/*.md lines 'traffic_bytes_per_cell_iter: X')."""
+    """DRAM bytes per cell and iteration that a committed ncu summary measured
+    for this workload (profiles/*.md lines
+    'traffic_bytes_per_cell_iter[<workload>]: X'); scaled to a launch by the
+    caller."""
+    key = f"traffic_bytes_per_cell_iter[{workload}]:"
     for p in sorted((ROOT / "profiles").glob("*.md")):
         for line in p.read_text().splitlines():
-            if line.startswith("traffic_bytes_per_cell_iter:"):
+            if line.startswith(key):
                 try:
                     return float(line.split(":", 1)[1].strip().split()[0]), p.name
                 except ValueError:

@@ -881,6 +881,23 @@ __device__ __noinline__ bool dist_tile(WarpSmem& w, int vt, int c, int z, unsign
 
 
 // ---- the persistent kernel ----------------------------------------------------
+// Phase trace (off unless a buffer is attached): two rows of 4 stamps
+// (%globaltimer ns) per HO iteration z: row 2z = [A start (min), A end (max),
+// LO start (min), LO end (max)], row 2z+1 = [C start (min), C end (max),
+// LO iterations, unused].
+__device__ __forceinline__ unsigned long long gtimer_h() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void trace_h(const HoloDev& P, int z, int slot, bool is_min) {
+    if (P.head.trace == nullptr || (threadIdx.x & 31) != 0 || 2 * z + 1 >= P.head.trace_iters)
+        return;
+    unsigned long long* p = P.head.trace + (size_t)8 * z + slot;
+    const unsigned long long t = gtimer_h();
+    if (is_min) atomicMin(p, t); else atomicMax(p, t);
+}
+
 __device__ __forceinline__ bool holo_sync(HoloDev& P, unsigned G) {
     if (grid_sync(&P.head.bar, G, &P.head.err, P.head.spin_limit)) return true;
     if (threadIdx.x == 0) atomicOr(&P.head.err_sticky, 1 << KEQ_ERR_TIMEOUT);
@@ -1132,6 +1149,7 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
         for (int b = 0; b < n_inst && !any; ++b) any = ho_active(P.inst[b], z);
         if (!any) break;
 
+        trace_h(P, z, 0, true);
         // A: Maxwellian partials of M(f_z); W_m = W_HO; boundary |Y| into max_YI
         for (long long t = gwarp; t < total_tiles; t += nwarps) {
             const int b = find_inst(P.tile_off, n_inst, t);
@@ -1148,6 +1166,8 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
         }
         if (!holo_sync(P, G)) return;
 
+        trace_h(P, z, 1, false);
+        trace_h(P, z, 2, true);
         // LO Picard iterations
         for (int m = 0; m < P.max_lo; ++m) {
             bool lany = false;
@@ -1193,6 +1213,13 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
             if (!holo_sync(P, G)) return;
         }
 
+        trace_h(P, z, 3, false);
+        if (P.head.trace && blockIdx.x == 0 && threadIdx.x == 0 && 2 * z + 1 < P.head.trace_iters) {
+            int nlo = 0;
+            while (nlo < P.max_lo && lo_active(P.inst[0], z, nlo)) ++nlo;
+            P.head.trace[(size_t)8 * z + 6] = (unsigned long long)nlo;
+        }
+        trace_h(P, z, 4, true);
         // C: distribution solve
         {
             const unsigned long long epoch = seq * (unsigned long long)(P.max_ho + 1) + z + 1;
@@ -1256,6 +1283,7 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
                 }
             }
         }
+        trace_h(P, z, 5, false);
         if (!holo_sync(P, G)) return;
     }
 

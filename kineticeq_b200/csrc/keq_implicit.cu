@@ -145,8 +145,10 @@ __device__ __forceinline__ bool inst_enabled(const ImpInst& I) {
 }
 
 __device__ __forceinline__ bool inst_active(const ImpInst& I, int m) {
-    if (m >= I.picard_iter) return false;
-    if (m == 0) return inst_enabled(I);
+    // A disabled instance's st/res hold a previous launch's values (the
+    // prologue skips it), so the mask is consulted at every iteration.
+    if (m >= I.picard_iter || !inst_enabled(I)) return false;
+    if (m == 0) return true;
     if (__ldcg(&I.st[m - 1]) != 1) return false;
     return !iter_done(I, m - 1);
 }
