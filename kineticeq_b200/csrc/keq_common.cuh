@@ -152,15 +152,29 @@ __device__ __forceinline__ double warp_max(double v) {
     return v;
 }
 
-// Grid barrier for a cooperative launch.  One arrival per CTA; the last
-// arriving CTA releases the generation word.  Every wait is bounded: on
-// timeout the CTA records KEQ_ERR_TIMEOUT in *err and the caller leaves its
-// loop.  The acquire load also invalidates the SM's L1, so ordinary loads
-// after the barrier observe other CTAs' stores made before it.
+// Grid barrier for a cooperative launch.  One arrival per CTA on a counter
+// that only grows within a launch (the host zeroes it before each launch):
+// the k-th barrier is passed once the counter reaches k * nblocks, and an
+// arriving CTA learns k from the value its own arrival returns (arrivals of
+// barrier k lie in [(k-1) nblocks, k nblocks) because no CTA can arrive at
+// barrier k+1 before barrier k is passed).  The arrival is a release and the
+// wait an acquire at gpu scope, so stores made by any thread of any CTA before
+// the barrier are visible to every thread after it (the CTA's bar.sync
+// carries the ordering to and from thread 0); the acquire also invalidates
+// the SM's L1 for the ordinary loads that follow.  No word is reset between
+// barriers, which saves the release round trip of a generation counter.
+// Every wait is bounded: on timeout the CTA records KEQ_ERR_TIMEOUT in *err
+// and the caller leaves its loop.
 struct GridBarrier {
     unsigned count;
-    unsigned gen;
+    unsigned pad;
 };
+
+__device__ __forceinline__ unsigned atom_add_release(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
 
 __device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned nblocks, int* err,
                                           unsigned long long limit = kSpinLimit) {
@@ -168,27 +182,21 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned nblocks, int
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        const unsigned g = ld_acquire(&gb->gen);
-        __threadfence();
-        const unsigned prev = atomicAdd(&gb->count, 1u);
-        if (prev == nblocks - 1) {
-            gb->count = 0u;
-            __threadfence();
-            st_release(&gb->gen, g + 1u);
-        } else {
+        const unsigned old = atom_add_release(&gb->count, 1u);
+        const unsigned target = (old / nblocks + 1u) * nblocks;
+        if (old + 1u != target) {
             unsigned long long it = 0;
-            unsigned ns = 32;
-            while (ld_acquire(&gb->gen) == g) {
+            unsigned ns = 0;
+            while ((int)(ld_acquire(&gb->count) - target) < 0) {
                 if (++it > limit) {
                     atomicOr(err, 1 << KEQ_ERR_TIMEOUT);
                     ok = 0;
                     break;
                 }
-                __nanosleep(ns);
-                if (ns < 256) ns <<= 1;
+                if (ns) __nanosleep(ns);
+                ns = ns ? (ns < 128 ? 2 * ns : ns) : 16;
             }
         }
-        __threadfence();
         s_ok = ok;
     }
     __syncthreads();

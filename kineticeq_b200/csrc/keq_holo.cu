@@ -881,19 +881,21 @@ __device__ __noinline__ bool dist_tile(WarpSmem& w, int vt, int c, int z, unsign
 
 
 // ---- the persistent kernel ----------------------------------------------------
-// Phase trace (off unless a buffer is attached): two rows of 4 stamps
-// (%globaltimer ns) per HO iteration z: row 2z = [A start (min), A end (max),
-// LO start (min), LO end (max)], row 2z+1 = [C start (min), C end (max),
-// LO iterations, unused].
+// Phase trace (off unless a buffer is attached): four rows of 4 stamps
+// (%globaltimer ns) per HO iteration z:
+//   row 4z   = [A start (min), A work end (max), LO start (min), LO end (max)]
+//   row 4z+1 = [C start (min), C work end (max), LO iterations, 0]
+//   row 4z+2 = LO iteration 0: [L1 start (min), L1 end (max), L2 start (min), L2 end (max)]
+//   row 4z+3 = LO iteration 0: [L3 start (min), L3 end (max), after its barrier (min), 0]
 __device__ __forceinline__ unsigned long long gtimer_h() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
 __device__ __forceinline__ void trace_h(const HoloDev& P, int z, int slot, bool is_min) {
-    if (P.head.trace == nullptr || (threadIdx.x & 31) != 0 || 2 * z + 1 >= P.head.trace_iters)
+    if (P.head.trace == nullptr || (threadIdx.x & 31) != 0 || 4 * z + 3 >= P.head.trace_iters)
         return;
-    unsigned long long* p = P.head.trace + (size_t)8 * z + slot;
+    unsigned long long* p = P.head.trace + (size_t)16 * z + slot;
     const unsigned long long t = gtimer_h();
     if (is_min) atomicMin(p, t); else atomicMax(p, t);
 }
@@ -1164,15 +1166,16 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
             for (int q = threadIdx.x; q < 3 * I.nx; q += kThreads) I.Wm[q] = __ldcg(&I.Who[q]);
             if (threadIdx.x == 0) atomic_max_nonneg(&I.ho_red[4 * z + 3], __ldcg(&I.misc[1]));
         }
+        trace_h(P, z, 1, false);
         if (!holo_sync(P, G)) return;
 
-        trace_h(P, z, 1, false);
         trace_h(P, z, 2, true);
         // LO Picard iterations
         for (int m = 0; m < P.max_lo; ++m) {
             bool lany = false;
             for (int b = 0; b < n_inst && !lany; ++b) lany = lo_active(P.inst[b], z, m);
             if (!lany) break;
+            if (m == 0) trace_h(P, z, 8, true);
             // L1
             for (long long u = gwarp; u < total_lo; u += nwarps) {
                 const int b = find_inst(P.lo_off, n_inst, u);
@@ -1190,7 +1193,9 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
                 }
                 lo_chunk_eliminate(w, kc);
             }
+            if (m == 0) trace_h(P, z, 9, false);
             if (!holo_sync(P, G)) return;
+            if (m == 0) trace_h(P, z, 10, true);
             // L2: one CTA per instance
             if (lane == 0) w.cur_b = -1;  // shared memory is reused below
             __syncthreads();
@@ -1202,7 +1207,9 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
             __syncthreads();
             if (lane == 0) w.cur_b = -1;
             __syncwarp();
+            if (m == 0) trace_h(P, z, 11, false);
             if (!holo_sync(P, G)) return;
+            if (m == 0) trace_h(P, z, 12, true);
             // L3
             for (long long u = gwarp; u < total_lo; u += nwarps) {
                 const int b = find_inst(P.lo_off, n_inst, u);
@@ -1210,14 +1217,16 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
                 if (!lo_active(w.I, z, m)) continue;
                 lo_chunk_recover(w, (int)(u - w.I.lo_off), z, m);
             }
+            if (m == 0) trace_h(P, z, 13, false);
             if (!holo_sync(P, G)) return;
+            if (m == 0) trace_h(P, z, 14, true);
         }
 
         trace_h(P, z, 3, false);
-        if (P.head.trace && blockIdx.x == 0 && threadIdx.x == 0 && 2 * z + 1 < P.head.trace_iters) {
+        if (P.head.trace && blockIdx.x == 0 && threadIdx.x == 0 && 4 * z + 3 < P.head.trace_iters) {
             int nlo = 0;
             while (nlo < P.max_lo && lo_active(P.inst[0], z, nlo)) ++nlo;
-            P.head.trace[(size_t)8 * z + 6] = (unsigned long long)nlo;
+            P.head.trace[(size_t)16 * z + 6] = (unsigned long long)nlo;
         }
         trace_h(P, z, 4, true);
         // C: distribution solve

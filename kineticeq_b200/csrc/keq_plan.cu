@@ -42,7 +42,7 @@ keq_status keq_plan_step(keq_plan* plan, int32_t n_steps, int32_t parity, keq_st
     if (cudaSetDevice(plan->device) != cudaSuccess) return cuda_fail(cudaGetLastError());
     for (int k = 0; k < n_steps; ++k) {
         int swap_io = ((parity + k) & 1);
-        // fresh barrier and error word for this launch (bar.count, bar.gen, err)
+        // fresh barrier counter and error word for this launch (bar.count, err)
         cudaError_t e = cudaMemsetAsync(plan->dev, 0, offsetof(keq::PlanHead, err_sticky), s);
         if (e != cudaSuccess) return cuda_fail(e);
         void* args[] = {&plan->dev, &swap_io};
