@@ -113,7 +113,6 @@ struct PlanDev {
 struct WarpSmem {
     ImpInst I;
     double a[kRmax][33];   // f^n tile -> c = b/d -> x (solution), row stride 33
-    double o[kRmax][32];   // f^(m) tile (residual reference)
     double coef[kRmax][4]; // (u, -1/(2T), n/sqrt(2 pi T), dt/tau) per row
     double vv[32];         // the tile's velocities (0 where absent)
     int cur_b, cur_m, cur_active, pad;
@@ -352,15 +351,22 @@ __device__ bool picard_tile(WarpSmem& w, int vt, int c, int m, unsigned long lon
     const TileGeo g = inst_tile(I, vt, c, lane);
     const int nx = I.nx, nv = I.nv;
     const int nr = g.nrows;
-    // f^n rows and the residual reference f^(m) (f^n itself at m = 0; the
-    // FP32 iterate after the FP32 sweeps of the mixed form)
+    // f^n rows into shared memory; the residual reference f^(m) (f^n itself
+    // at m = 0; the FP32 iterate after the FP32 sweeps of the mixed form) is
+    // streamed into registers 8 rows ahead of the recurrence, the first 8
+    // rows before the look-back
     const bool ref32 = m > 0 && fp32_iter(I, m - 1);
+    const double* ref64 = m > 0 ? fo : fn;
     stage_rows<33>(w.a, fn, g, nx, nv);
-    if (!ref32) stage_rows<32>(w.o, m > 0 ? fo : fn, g, nx, nv);
     cp_async_commit();
-    if (ref32 && g.lane_ok)
-        for (int r = 0; r < nr; ++r)
-            w.o[r][lane] = (double)__ldcg(&I.x32[(size_t)scan_row(nx, g.pos, g.s0 + r) * nv + g.j]);
+    auto ld_ref = [&](int r) -> double {
+        if (r >= nr || !g.lane_ok) return 0.0;
+        const size_t off = (size_t)scan_row(nx, g.pos, g.s0 + r) * nv + g.j;
+        return ref32 ? (double)__ldcg(&I.x32[off]) : __ldcg(&ref64[off]);
+    };
+    double on[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) on[t] = ld_ref(t);
     const double vj = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
     w.vv[lane] = vj;
     stage_coeffs(w, g, vt, m);
@@ -406,20 +412,31 @@ __device__ bool picard_tile(WarpSmem& w, int vt, int c, int m, unsigned long lon
     if (c + 1 < I.nchunks) publish_inc(I.inc, I.flag, tid, fma(P, X, Y), epoch);
     // recurrence, write, residual
     const double tol = I.tol, abs_tol = I.abs_tol;
-#pragma unroll 4
-    for (int r = 0; r < nr; ++r) {
-        const double a = cpl * recip_ge1(one_plus + w.coef[r][3]);
-        X = fma(a, X, w.a[r][lane]);
-        const double x = g.lane_ok ? X : 0.0;
-        w.a[r][lane] = x;
-        if (g.lane_ok) {
-            const double o = w.o[r][lane];
-            const double df = fabs(x - o);
-            const double ref = nan_max(fabs(x), fabs(o));
-            q1.add(df, abs_tol + tol * ref);
-            q2.add(df, (ref != ref || ref >= abs_tol) ? ref : abs_tol);
-            bad |= !isfinite(x);
+#pragma unroll 1
+    for (int r0 = 0; r0 < nr; r0 += 8) {
+        double onx[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) onx[t] = ld_ref(r0 + 8 + t);
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const int r = r0 + t;
+            if (r < nr) {
+                const double a = cpl * recip_ge1(one_plus + w.coef[r][3]);
+                X = fma(a, X, w.a[r][lane]);
+                const double x = g.lane_ok ? X : 0.0;
+                w.a[r][lane] = x;
+                if (g.lane_ok) {
+                    const double o = on[t];
+                    const double df = fabs(x - o);
+                    const double ref = nan_max(fabs(x), fabs(o));
+                    q1.add(df, abs_tol + tol * ref);
+                    q2.add(df, (ref != ref || ref >= abs_tol) ? ref : abs_tol);
+                    bad |= !isfinite(x);
+                }
+            }
         }
+#pragma unroll
+        for (int t = 0; t < 8; ++t) on[t] = onx[t];
     }
     store_partials(w, g, vt);
     return ok;
@@ -443,18 +460,25 @@ __device__ bool picard_tile32(WarpSmem& w, int vt, int c, int m, unsigned long l
     const TileGeo g = inst_tile(I, vt, c, lane);
     const int nx = I.nx, nv = I.nv;
     const int nr = g.nrows;
-    float(*fa)[32] = reinterpret_cast<float(*)[32]>(&w.o[0][0]);  // f^n (FP32)
-    float(*fb)[32] = fa + kRmax;                                   // previous iterate
+    // f^n (FP32) staged in the tile buffer (read into registers by the map
+    // loop before the recurrence writes the buffer); the previous FP32
+    // iterate streamed into registers
+    float(*fa)[32] = reinterpret_cast<float(*)[32]>(&w.a[0][0]);
     const float* ref = m > 0 ? I.x32 : I.fn32;
     if (g.lane_ok) {
 #pragma unroll 8
         for (int r = 0; r < nr; ++r) {
             const size_t off = (size_t)scan_row(nx, g.pos, g.s0 + r) * nv + g.j;
             cp_async4(&fa[r][lane], I.fn32 + off);
-            cp_async4(&fb[r][lane], ref + off);
         }
     }
     cp_async_commit();
+    float fbv[kRmax];
+#pragma unroll
+    for (int r = 0; r < kRmax; ++r)
+        fbv[r] = (r < nr && g.lane_ok)
+                     ? __ldcg(&ref[(size_t)scan_row(nx, g.pos, g.s0 + r) * nv + g.j])
+                     : 0.0f;
     const double vjd = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
     w.vv[lane] = vjd;
     stage_coeffs(w, g, vt, m);
@@ -491,6 +515,7 @@ __device__ bool picard_tile32(WarpSmem& w, int vt, int c, int m, unsigned long l
         ok = lookback(I.agg, I.inc, I.flag, I.nvt, vt, c, epoch, limit, Xd);
     }
     if (c + 1 < I.nchunks) publish_inc(I.inc, I.flag, tid, fma((double)P, Xd, (double)Y), epoch);
+    __syncwarp();  // every lane has read its f^n (FP32) before the buffer takes x
     float X = (float)Xd;
     const double tol = I.tol32, abs_tol = I.abs_tol;
 #pragma unroll
@@ -501,7 +526,7 @@ __device__ bool picard_tile32(WarpSmem& w, int vt, int c, int m, unsigned long l
             const float x = g.lane_ok ? X : 0.0f;
             w.a[r][lane] = (double)x;
             if (g.lane_ok) {
-                const double o = (double)fb[r][lane];
+                const double o = (double)fbv[r];
                 const double df = fabs((double)x - o);
                 const double rf = nan_max(fabs((double)x), fabs(o));
                 q1.add(df, abs_tol + tol * rf);
@@ -869,7 +894,7 @@ __device__ __forceinline__ long long claim(unsigned* tickets, int m) {
 // The Picard pass claims tiles from a ticket counter so tiles are started in
 // x order (chunk-major), which keeps every look-back short and guarantees
 // that a tile's predecessors are held by running warps.
-__global__ void __launch_bounds__(kThreads, 3)
+__global__ void __launch_bounds__(kThreads, 4)
 implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     PlanDev& P = *Pp;
