@@ -57,8 +57,8 @@ namespace holo {
 constexpr int kWarps = 4;
 constexpr int kThreads = kWarps * 32;
 constexpr double kTheta = 0.5;
-constexpr int kMaxLoChunk = 64;     // rows per LO chunk at most
-constexpr int kMaxLoChunks = 248;   // LO chunks per instance at most (PCR in shared memory)
+constexpr int kLoChunk = 32;        // rows per LO chunk (one per lane)
+constexpr int kMaxLoChunks = 512;   // LO chunks per instance at most (16 groups of 32)
 
 struct HoloInst {
     int nx, nv, n_inner, kp;
@@ -478,263 +478,392 @@ __device__ __noinline__ double lo_prep_row(const HoloInst& I, int k) {
     return mx;
 }
 
-// L1: block rows of one LO chunk into shared memory (lane-parallel), local
-// elimination of rows s..e-1 (lane 0: (n, nu) 2x2 blocks, lane 1: U), and
-// the representation x_i = y_i + P_i xi_{k-1} + Q_i xi_k of every row of the
-// chunk (last row: y = 0, P = 0, Q = I) into lorow; the chunk's last block
-// row into loedge.
+// ---- LO: warp-parallel block PCR ---------------------------------------------
+// One block row per lane of a block-tridiagonal system with 2x2 blocks for
+// (n, nu) and a scalar system for U:
+//     A x_{l-1} + B x_l + C x_{l+1} = R,   a u_{l-1} + b u_l + c u_{l+1} = r,
+// R holding 5 right-hand-side columns (2 x 5, row-major) and r 3.  Parallel
+// cyclic reduction over the lanes: at stride d every row eliminates its
+// couplings to rows l-d and l+d with their (pre-step) blocks, fetched by
+// shuffles; after log2(L) steps every row is decoupled and B^{-1} R, r / b
+// are the solution columns.  Lanes >= L carry identity rows.
+struct PcrRow {
+    double A[4], B[4], C[4], R[10];
+    double a, b, c, r[3];
+};
+
+__device__ __forceinline__ double shup(double v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
+__device__ __forceinline__ double shdn(double v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+
+__device__ __forceinline__ void identity_row(PcrRow& q) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        q.A[k] = 0.0;
+        q.C[k] = 0.0;
+        q.B[k] = (k == 0 || k == 3) ? 1.0 : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < 10; ++k) q.R[k] = 0.0;
+    q.a = 0.0; q.b = 1.0; q.c = 0.0;
+    q.r[0] = q.r[1] = q.r[2] = 0.0;
+}
+
+__device__ __forceinline__ void warp_pcr(PcrRow& q, int L) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll 1
+    for (int d = 1; d < L; d <<= 1) {
+        double Bi[4];
+        inv2(q.B, Bi);
+        const double bi = rcp_or0(q.b);
+        const bool has_lo = lane >= d && lane < L, has_hi = lane + d < L;
+        double nA[4], nC[4], dB[4], nR[10];
+        double na, nc, db, nr[3];
+        // lower neighbour: alpha = -A B_lo^{-1}
+        {
+            double t[4], al[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) t[k] = shup(Bi[k], d);
+            mm2(q.A, t, al);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) al[k] = has_lo ? -al[k] : 0.0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) t[k] = shup(q.A[k], d);
+            mm2(al, t, nA);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) t[k] = shup(q.C[k], d);
+            mm2(al, t, dB);
+#pragma unroll
+            for (int j = 0; j < 5; ++j) {
+                const double r0 = shup(q.R[j], d), r1 = shup(q.R[5 + j], d);
+                nR[j] = q.R[j] + (al[0] * r0 + al[1] * r1);
+                nR[5 + j] = q.R[5 + j] + (al[2] * r0 + al[3] * r1);
+            }
+            const double bl = shup(bi, d);  // every lane shuffles; the mask is the full warp
+            const double a1 = has_lo ? -q.a * bl : 0.0;
+            na = a1 * shup(q.a, d);
+            db = a1 * shup(q.c, d);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) nr[j] = q.r[j] + a1 * shup(q.r[j], d);
+        }
+        // upper neighbour: gamma = -C B_hi^{-1}
+        {
+            double t[4], ga[4], u[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) t[k] = shdn(Bi[k], d);
+            mm2(q.C, t, ga);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) ga[k] = has_hi ? -ga[k] : 0.0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) t[k] = shdn(q.C[k], d);
+            mm2(ga, t, nC);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) t[k] = shdn(q.A[k], d);
+            mm2(ga, t, u);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) dB[k] += u[k];
+#pragma unroll
+            for (int j = 0; j < 5; ++j) {
+                const double r0 = shdn(q.R[j], d), r1 = shdn(q.R[5 + j], d);
+                nR[j] += ga[0] * r0 + ga[1] * r1;
+                nR[5 + j] += ga[2] * r0 + ga[3] * r1;
+            }
+            const double bh = shdn(bi, d);
+            const double g1 = has_hi ? -q.c * bh : 0.0;
+            nc = g1 * shdn(q.c, d);
+            db += g1 * shdn(q.a, d);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) nr[j] += g1 * shdn(q.r[j], d);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            q.A[k] = nA[k];
+            q.C[k] = nC[k];
+            q.B[k] += dB[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 10; ++k) q.R[k] = nR[k];
+        q.a = na;
+        q.c = nc;
+        q.b += db;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) q.r[j] = nr[j];
+    }
+    double Bi[4];
+    inv2(q.B, Bi);
+    double nR[10];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+        nR[j] = Bi[0] * q.R[j] + Bi[1] * q.R[5 + j];
+        nR[5 + j] = Bi[2] * q.R[j] + Bi[3] * q.R[5 + j];
+    }
+#pragma unroll
+    for (int k = 0; k < 10; ++k) q.R[k] = nR[k];
+    const double bi = rcp_or0(q.b);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) q.r[j] *= bi;
+}
+
+// Solution columns [y | P | Q] of a PCR row as the 13-value representation
+// y(2) y_U | P(2x2) P_U | Q(2x2) Q_U of x = y + P x_left + Q x_right.
+__device__ __forceinline__ void rep_of(const PcrRow& q, double* o) {
+    o[0] = q.R[0]; o[1] = q.R[5]; o[2] = q.r[0];
+    o[3] = q.R[1]; o[4] = q.R[2]; o[5] = q.R[6]; o[6] = q.R[7]; o[7] = q.r[1];
+    o[8] = q.R[3]; o[9] = q.R[4]; o[10] = q.R[8]; o[11] = q.R[9]; o[12] = q.r[2];
+}
+
+// Local system of L rows (lane l = row l, couplings A_l, C_l) with the
+// left coupling of row 0 and the right coupling of row L-1 moved to the
+// right-hand side as the P and Q columns (D, -A_0 e_0, -C_{L-1} e_{L-1}).
+__device__ __forceinline__ void local_rows(PcrRow& q, const double* A, const double* B,
+                                           const double* C, const double* D, double a, double b,
+                                           double c, double d, int l, int L) {
+    if (l >= L) {
+        identity_row(q);
+        return;
+    }
+    const bool first = l == 0, last = l == L - 1;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        q.A[k] = first ? 0.0 : A[k];
+        q.B[k] = B[k];
+        q.C[k] = last ? 0.0 : C[k];
+    }
+    q.R[0] = D[0];
+    q.R[5] = D[1];
+    q.R[1] = first ? -A[0] : 0.0; q.R[2] = first ? -A[1] : 0.0;
+    q.R[6] = first ? -A[2] : 0.0; q.R[7] = first ? -A[3] : 0.0;
+    q.R[3] = last ? -C[0] : 0.0; q.R[4] = last ? -C[1] : 0.0;
+    q.R[8] = last ? -C[2] : 0.0; q.R[9] = last ? -C[3] : 0.0;
+    q.a = first ? 0.0 : a;
+    q.b = b;
+    q.c = last ? 0.0 : c;
+    q.r[0] = d;
+    q.r[1] = first ? -a : 0.0;
+    q.r[2] = last ? -c : 0.0;
+}
+
+// L1: block rows of one LO chunk (lane = row; rows s..e, e the chunk's
+// interface row), the warp-parallel solve of the local rows s..e-1 into the
+// representation x_r = y_r + P_r xi_{k-1} + Q_r xi_k (row e: y = 0, P = 0,
+// Q = I) in lorow, and the interface row's blocks in loedge.
 __device__ __noinline__ void lo_chunk_eliminate(WarpSmem& w, int kc) {
     const HoloInst& I = w.I;
     const int lane = threadIdx.x & 31;
     const int s = kc * I.lo_len;
     const int e = (s + I.lo_len < I.n_inner ? s + I.lo_len : I.n_inner) - 1;
     const int len = e - s + 1;
-    LoRow* rows = reinterpret_cast<LoRow*>(&w.a[0][0]);  // kMaxLoChunk rows fit in w.a + w.o
-    for (int r = lane; r < len; r += 32) lo_row(I, s + r, rows[r]);
-    __syncwarp();
-    // last block row of the chunk -> loedge
-    if (lane < 18) {
-        const LoRow& L = rows[len - 1];
-        const double vals[18] = {L.A[0], L.A[1], L.A[2], L.A[3], L.B[0], L.B[1], L.B[2], L.B[3],
-                                 L.C[0], L.C[1], L.C[2], L.C[3], L.D[0], L.D[1],
-                                 L.a, L.b, L.c, L.d};
-        I.loedge[(size_t)kc * 18 + lane] = vals[lane];
-    }
-    // per-row outputs, staged in the o/coef area after the row blocks
-    double* outp = reinterpret_cast<double*>(&rows[kMaxLoChunk]);  // 13 per row
-    const int nloc = len - 1;  // rows s..e-1 eliminated locally
-    if (lane == 0 && nloc > 0) {
-        // forward sweep with C' and R' = [y | P (2 cols) | Q (2 cols)] stored per row
-        double Cp[4], Ry[2], RP[4], RQ[4];
-        for (int r = 0; r < nloc; ++r) {
-            const LoRow& L = rows[r];
-            double M[4], ry[2], rP[4], rQ[4];
-            if (r == 0) {
-                M[0] = L.B[0]; M[1] = L.B[1]; M[2] = L.B[2]; M[3] = L.B[3];
-                ry[0] = L.D[0]; ry[1] = L.D[1];
-                rP[0] = -L.A[0]; rP[1] = -L.A[1]; rP[2] = -L.A[2]; rP[3] = -L.A[3];
-                rQ[0] = rQ[1] = rQ[2] = rQ[3] = 0.0;
-            } else {
-                double T4[4], t2[2];
-                mm2(L.A, Cp, T4);
-                M[0] = L.B[0] - T4[0]; M[1] = L.B[1] - T4[1]; M[2] = L.B[2] - T4[2]; M[3] = L.B[3] - T4[3];
-                mv2(L.A, Ry, t2);
-                ry[0] = L.D[0] - t2[0]; ry[1] = L.D[1] - t2[1];
-                mm2(L.A, RP, T4);
-                rP[0] = -T4[0]; rP[1] = -T4[1]; rP[2] = -T4[2]; rP[3] = -T4[3];
-                mm2(L.A, RQ, T4);
-                rQ[0] = -T4[0]; rQ[1] = -T4[1]; rQ[2] = -T4[2]; rQ[3] = -T4[3];
-            }
-            if (r == nloc - 1) {  // coupling to the chunk's last row moves to the RHS
-                rQ[0] -= L.C[0]; rQ[1] -= L.C[1]; rQ[2] -= L.C[2]; rQ[3] -= L.C[3];
-            }
-            double Mi[4];
-            inv2(M, Mi);
-            mv2(Mi, ry, Ry);
-            mm2(Mi, rP, RP);
-            mm2(Mi, rQ, RQ);
-            if (r < nloc - 1) mm2(Mi, L.C, Cp);
-            double* o = outp + 13 * r;
-            o[0] = Ry[0]; o[1] = Ry[1];
-            o[3] = RP[0]; o[4] = RP[1]; o[5] = RP[2]; o[6] = RP[3];
-            o[8] = RQ[0]; o[9] = RQ[1]; o[10] = RQ[2]; o[11] = RQ[3];
-            // keep C'_r for the backward sweep in the row's (now unused) A slot
-            if (r < nloc - 1) {
-                rows[r].A[0] = Cp[0]; rows[r].A[1] = Cp[1]; rows[r].A[2] = Cp[2]; rows[r].A[3] = Cp[3];
-            }
-        }
-        // backward: x_r = R'_r - C'_r x_{r+1}
-        for (int r = nloc - 2; r >= 0; --r) {
-            const double* Cr = rows[r].A;
-            double* o = outp + 13 * r;
-            const double* on = outp + 13 * (r + 1);
-            double t2[2], T4[4];
-            const double yn[2] = {on[0], on[1]};
-            mv2(Cr, yn, t2);
-            o[0] -= t2[0]; o[1] -= t2[1];
-            const double Pn[4] = {on[3], on[4], on[5], on[6]};
-            mm2(Cr, Pn, T4);
-            o[3] -= T4[0]; o[4] -= T4[1]; o[5] -= T4[2]; o[6] -= T4[3];
-            const double Qn[4] = {on[8], on[9], on[10], on[11]};
-            mm2(Cr, Qn, T4);
-            o[8] -= T4[0]; o[9] -= T4[1]; o[10] -= T4[2]; o[11] -= T4[3];
-        }
-    }
-    if (lane == 1 && nloc > 0) {
-        double cp = 0.0, ry = 0.0, rp = 0.0, rq = 0.0;
-        for (int r = 0; r < nloc; ++r) {
-            const LoRow& L = rows[r];
-            double m, y0, p0, q0;
-            if (r == 0) {
-                m = L.b; y0 = L.d; p0 = -L.a; q0 = 0.0;
-            } else {
-                m = L.b - L.a * cp; y0 = L.d - L.a * ry; p0 = -(L.a * rp); q0 = -(L.a * rq);
-            }
-            if (r == nloc - 1) q0 -= L.c;
-            const double mi = rcp_or0(m);
-            ry = mi * y0; rp = mi * p0; rq = mi * q0;
-            double* o = outp + 13 * r;
-            o[2] = ry; o[7] = rp; o[12] = rq;
-            cp = (r < nloc - 1) ? mi * L.c : 0.0;
-            rows[r].cu = cp;
-        }
-        for (int r = nloc - 2; r >= 0; --r) {
-            const double cr = rows[r].cu;
-            double* o = outp + 13 * r;
-            const double* on = outp + 13 * (r + 1);
-            o[2] -= cr * on[2];
-            o[7] -= cr * on[7];
-            o[12] -= cr * on[12];
-        }
-    }
-    __syncwarp();
-    // rows s..e-1: computed; row e: y = 0, P = 0, Q = I
-    for (int r = lane; r < len; r += 32) {
-        double* dst = I.lorow + 13 * (size_t)(s + r);
-        if (r < nloc) {
-            const double* o = outp + 13 * r;
+    const int nloc = len - 1;  // rows s..e-1 solved locally
+    LoRow L{};
+    if (lane < len) lo_row(I, s + lane, L);
+    if (lane == nloc) {
+        double* ed = I.loedge + (size_t)kc * 18;
 #pragma unroll
-            for (int q = 0; q < 13; ++q) dst[q] = o[q];
+        for (int k = 0; k < 4; ++k) {
+            ed[k] = L.A[k];
+            ed[4 + k] = L.B[k];
+            ed[8 + k] = L.C[k];
+        }
+        ed[12] = L.D[0]; ed[13] = L.D[1];
+        ed[14] = L.a; ed[15] = L.b; ed[16] = L.c; ed[17] = L.d;
+    }
+    PcrRow q;
+    local_rows(q, L.A, L.B, L.C, L.D, L.a, L.b, L.c, L.d, lane, nloc);
+    warp_pcr(q, nloc);
+    if (lane < len) {
+        double o[13];
+        if (lane < nloc) {
+            rep_of(q, o);
         } else {
 #pragma unroll
-            for (int q = 0; q < 13; ++q) dst[q] = 0.0;
-            dst[8] = 1.0; dst[11] = 1.0; dst[12] = 1.0;
+            for (int k = 0; k < 13; ++k) o[k] = 0.0;
+            o[8] = 1.0; o[11] = 1.0; o[12] = 1.0;
         }
+        double* dst = I.lorow + 13 * (size_t)(s + lane);
+#pragma unroll
+        for (int k = 0; k < 13; ++k) dst[k] = o[k];
     }
 }
 
-// Representation (y, P, Q) of the row before row `row0` for chunk kc's
-// interface equation: row e-1 of chunk kc if the chunk has 2+ rows, else the
-// previous chunk's interface unknown itself (y = 0, P = I, Q = 0).
+// Representation (y, P, Q) of a row: from lorow, or the identity forms
+// (y = 0, P = I, Q = 0: the previous interface itself; all zero: absent).
 __device__ __forceinline__ void rep_load(const double* lr, double* o13) {
 #pragma unroll
     for (int q = 0; q < 13; ++q) o13[q] = __ldcg(&lr[q]);
 }
 
-// L2: the reduced system on the K interface unknowns xi_k (last row of every
-// chunk), one CTA per instance, by parallel cyclic reduction in shared memory:
+// Interface row of chunk k (its last row e):
 //   alpha_k xi_{k-1} + beta_k xi_k + gamma_k xi_{k+1} = delta_k,
 //   alpha = A_e P_{e-1}, beta = B_e + A_e Q_{e-1} + C_e P_{s'},
-//   gamma = C_e Q_{s'}, delta = D_e - A_e y_{e-1} - C_e y_{s'}.
-struct Red2 { double al[4], be[4], ga[4], de[2]; };
-struct Red1 { double al, be, ga, de; };
+//   gamma = C_e Q_{s'}, delta = D_e - A_e y_{e-1} - C_e y_{s'}
+// (s' the first row of chunk k+1), the same for the U scalar.
+__device__ __forceinline__ void interface_row(const HoloInst& I, int k, double* al, double* be,
+                                              double* ga, double* de, double* s4) {
+    const int s = k * I.lo_len;
+    const int e = (s + I.lo_len < I.n_inner ? s + I.lo_len : I.n_inner) - 1;
+    double ed[18];
+#pragma unroll
+    for (int q = 0; q < 18; ++q) ed[q] = __ldcg(&I.loedge[(size_t)k * 18 + q]);
+    const double* A = ed; const double* B = ed + 4; const double* C = ed + 8;
+    const double* D = ed + 12;
+    double pm[13], nx_[13];
+    if (e > s) {
+        rep_load(I.lorow + 13 * (size_t)(e - 1), pm);
+    } else {
+#pragma unroll
+        for (int q = 0; q < 13; ++q) pm[q] = 0.0;
+        pm[3] = 1.0; pm[6] = 1.0; pm[7] = 1.0;
+    }
+    if (k + 1 < I.lo_k) {
+        rep_load(I.lorow + 13 * (size_t)(e + 1), nx_);
+    } else {
+#pragma unroll
+        for (int q = 0; q < 13; ++q) nx_[q] = 0.0;
+    }
+    double T4[4], U4[4], t2[2], u2[2];
+    mm2(A, pm + 3, al);
+    mm2(A, pm + 8, T4);
+    mm2(C, nx_ + 3, U4);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) be[q] = B[q] + T4[q] + U4[q];
+    mm2(C, nx_ + 8, ga);
+    mv2(A, pm, t2);
+    mv2(C, nx_, u2);
+    de[0] = D[0] - t2[0] - u2[0];
+    de[1] = D[1] - t2[1] - u2[1];
+    const double a = ed[14], b = ed[15], c = ed[16], d = ed[17];
+    s4[0] = a * pm[7];
+    s4[1] = b + a * pm[12] + c * nx_[7];
+    s4[2] = c * nx_[12];
+    s4[3] = d - a * pm[2] - c * nx_[2];
+}
+
+// L2: the interface system of the K = lo_k chunks, one CTA per instance.
+// The interface rows are split into groups of 32; each group is solved by
+// warp PCR into xi_k = y_k + P_k X_{g-1} + Q_k X_g in terms of the group
+// interfaces X_g (the last interface of every group), whose own system (at
+// most 32 unknowns) is solved by warp 0 the same way; then every xi_k is
+// recovered into I.xi.
+struct GroupRec {
+    double rep_prev[13];  // representation of the group row before the last
+    double rep_first[13]; // representation of the group's first row
+    double al[4], be[4], ga[4], de[2], s4[4];  // the group's last interface row
+};
 
 __device__ __noinline__ void lo_reduced_solve(const HoloInst& I, unsigned char* smem) {
     const int K = I.lo_k;
-    Red2* b2[2] = {reinterpret_cast<Red2*>(smem), reinterpret_cast<Red2*>(smem) + K};
-    Red1* b1[2] = {reinterpret_cast<Red1*>(smem + 2 * sizeof(Red2) * K),
-                   reinterpret_cast<Red1*>(smem + 2 * sizeof(Red2) * K) + K};
-    for (int k = threadIdx.x; k < K; k += blockDim.x) {
-        const int s = k * I.lo_len;
-        const int e = (s + I.lo_len < I.n_inner ? s + I.lo_len : I.n_inner) - 1;
-        double ed[18];
-#pragma unroll
-        for (int q = 0; q < 18; ++q) ed[q] = __ldcg(&I.loedge[(size_t)k * 18 + q]);
-        const double* A = ed; const double* B = ed + 4; const double* C = ed + 8;
-        const double* D = ed + 12;
-        double pm[13], nx_[13];
-        if (e > s) {
-            rep_load(I.lorow + 13 * (size_t)(e - 1), pm);
+    const int G = (K + 31) / 32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    GroupRec* grec = reinterpret_cast<GroupRec*>(smem);
+    double* reps = reinterpret_cast<double*>(smem + sizeof(GroupRec) * G);  // K x 13
+    double* X = reps + 13 * (size_t)K;                                      // G x 3
+    for (int g = warp; g < G; g += kWarps) {
+        const int k0 = 32 * g;
+        const int len = (K - k0) < 32 ? (K - k0) : 32;
+        const int nloc = len - 1;
+        const int k = k0 + lane;
+        double al[4] = {0, 0, 0, 0}, be[4] = {1, 0, 0, 1}, ga[4] = {0, 0, 0, 0}, de[2] = {0, 0};
+        double s4[4] = {0.0, 1.0, 0.0, 0.0};
+        if (lane < len) interface_row(I, k, al, be, ga, de, s4);
+        PcrRow q;
+        local_rows(q, al, be, ga, de, s4[0], s4[1], s4[2], s4[3], lane, nloc);
+        warp_pcr(q, nloc);
+        double o[13];
+        if (lane < nloc) {
+            rep_of(q, o);
         } else {
 #pragma unroll
-            for (int q = 0; q < 13; ++q) pm[q] = 0.0;
-            pm[3] = 1.0; pm[6] = 1.0; pm[7] = 1.0;
+            for (int t = 0; t < 13; ++t) o[t] = 0.0;
+            o[8] = 1.0; o[11] = 1.0; o[12] = 1.0;
         }
-        const bool has_next = k + 1 < K;
-        if (has_next) {
-            rep_load(I.lorow + 13 * (size_t)(e + 1), nx_);
-        } else {
+        if (lane < len) {
 #pragma unroll
-            for (int q = 0; q < 13; ++q) nx_[q] = 0.0;
+            for (int t = 0; t < 13; ++t) reps[13 * (size_t)k + t] = o[t];
         }
-        Red2 r2;
-        double T4[4], U4[4], t2[2], u2[2];
-        mm2(A, pm + 3, r2.al);
-        mm2(A, pm + 8, T4);
-        mm2(C, nx_ + 3, U4);
-        for (int q = 0; q < 4; ++q) r2.be[q] = B[q] + T4[q] + U4[q];
-        mm2(C, nx_ + 8, r2.ga);
-        mv2(A, pm, t2);
-        mv2(C, nx_, u2);
-        r2.de[0] = D[0] - t2[0] - u2[0];
-        r2.de[1] = D[1] - t2[1] - u2[1];
-        b2[0][k] = r2;
-        Red1 r1;
-        const double a = ed[14], b = ed[15], c = ed[16], d = ed[17];
-        r1.al = a * pm[7];
-        r1.be = b + a * pm[12] + c * nx_[7];
-        r1.ga = c * nx_[12];
-        r1.de = d - a * pm[2] - c * nx_[2];
-        b1[0][k] = r1;
+        if (lane == nloc) {
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                grec[g].al[t] = al[t];
+                grec[g].be[t] = be[t];
+                grec[g].ga[t] = ga[t];
+                grec[g].s4[t] = s4[t];
+            }
+            grec[g].de[0] = de[0];
+            grec[g].de[1] = de[1];
+        }
+        __syncwarp();
+        if (lane < 13) {
+            grec[g].rep_first[lane] = reps[13 * (size_t)k0 + lane];
+            grec[g].rep_prev[lane] = (nloc >= 1) ? reps[13 * (size_t)(k0 + nloc - 1) + lane]
+                                                 : ((lane == 3 || lane == 6 || lane == 7) ? 1.0 : 0.0);
+        }
     }
     __syncthreads();
-    int cur = 0;
-    for (int sd = 1; sd < K; sd <<= 1) {
-        for (int k = threadIdx.x; k < K; k += blockDim.x) {
-            const Red2& me = b2[cur][k];
-            Red2 nw = me;
-            if (k - sd >= 0) {
-                const Red2& lo = b2[cur][k - sd];
-                double bi[4], e1[4], T4[4], t2[2];
-                inv2(lo.be, bi);
-                mm2(me.al, bi, e1);
-                mm2(e1, lo.al, T4);
-                for (int q = 0; q < 4; ++q) nw.al[q] = -T4[q];
-                mm2(e1, lo.ga, T4);
-                for (int q = 0; q < 4; ++q) nw.be[q] -= T4[q];
-                mv2(e1, lo.de, t2);
-                nw.de[0] -= t2[0]; nw.de[1] -= t2[1];
-            } else {
-                for (int q = 0; q < 4; ++q) nw.al[q] = 0.0;
-            }
-            if (k + sd < K) {
-                const Red2& hi = b2[cur][k + sd];
-                double bi[4], e2[4], T4[4], t2[2];
-                inv2(hi.be, bi);
-                mm2(me.ga, bi, e2);
-                mm2(e2, hi.ga, T4);
-                for (int q = 0; q < 4; ++q) nw.ga[q] = -T4[q];
-                mm2(e2, hi.al, T4);
-                for (int q = 0; q < 4; ++q) nw.be[q] -= T4[q];
-                mv2(e2, hi.de, t2);
-                nw.de[0] -= t2[0]; nw.de[1] -= t2[1];
-            } else {
-                for (int q = 0; q < 4; ++q) nw.ga[q] = 0.0;
-            }
-            b2[cur ^ 1][k] = nw;
-            const Red1& m1 = b1[cur][k];
-            Red1 n1 = m1;
-            if (k - sd >= 0) {
-                const Red1& lo = b1[cur][k - sd];
-                const double e1 = m1.al * rcp_or0(lo.be);
-                n1.al = -(e1 * lo.al);
-                n1.be -= e1 * lo.ga;
-                n1.de -= e1 * lo.de;
-            } else {
-                n1.al = 0.0;
-            }
-            if (k + sd < K) {
-                const Red1& hi = b1[cur][k + sd];
-                const double e2 = m1.ga * rcp_or0(hi.be);
-                n1.ga = -(e2 * hi.ga);
-                n1.be -= e2 * hi.al;
-                n1.de -= e2 * hi.de;
-            } else {
-                n1.ga = 0.0;
-            }
-            b1[cur ^ 1][k] = n1;
+    // group interfaces: the same interface-row construction one level up
+    if (warp == 0) {
+        double A[4] = {0, 0, 0, 0}, B[4] = {1, 0, 0, 1}, C[4] = {0, 0, 0, 0}, D[2] = {0, 0};
+        double a = 0.0, b = 1.0, c = 0.0, d = 0.0;
+        if (lane < G) {
+            const GroupRec& gr = grec[lane];
+            const double* pm = gr.rep_prev;
+            double nx_[13];
+#pragma unroll
+            for (int t = 0; t < 13; ++t) nx_[t] = (lane + 1 < G) ? grec[lane + 1].rep_first[t] : 0.0;
+            double T4[4], U4[4], t2[2], u2[2];
+            mm2(gr.al, pm + 3, A);
+            mm2(gr.al, pm + 8, T4);
+            mm2(gr.ga, nx_ + 3, U4);
+#pragma unroll
+            for (int t = 0; t < 4; ++t) B[t] = gr.be[t] + T4[t] + U4[t];
+            mm2(gr.ga, nx_ + 8, C);
+            mv2(gr.al, pm, t2);
+            mv2(gr.ga, nx_, u2);
+            D[0] = gr.de[0] - t2[0] - u2[0];
+            D[1] = gr.de[1] - t2[1] - u2[1];
+            a = gr.s4[0] * pm[7];
+            b = gr.s4[1] + gr.s4[0] * pm[12] + gr.s4[2] * nx_[7];
+            c = gr.s4[2] * nx_[12];
+            d = gr.s4[3] - gr.s4[0] * pm[2] - gr.s4[2] * nx_[2];
         }
-        __syncthreads();
-        cur ^= 1;
+        PcrRow q;
+        if (lane < G) {
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                q.A[t] = A[t];
+                q.B[t] = B[t];
+                q.C[t] = C[t];
+            }
+#pragma unroll
+            for (int t = 0; t < 10; ++t) q.R[t] = 0.0;
+            q.R[0] = D[0];
+            q.R[5] = D[1];
+            q.a = a; q.b = b; q.c = c;
+            q.r[0] = d; q.r[1] = 0.0; q.r[2] = 0.0;
+        } else {
+            identity_row(q);
+        }
+        warp_pcr(q, G);
+        if (lane < G) {
+            X[3 * lane + 0] = q.R[0];
+            X[3 * lane + 1] = q.R[5];
+            X[3 * lane + 2] = q.r[0];
+        }
     }
+    __syncthreads();
+    // every interface unknown from its group representation
     for (int k = threadIdx.x; k < K; k += blockDim.x) {
-        const Red2& r = b2[cur][k];
-        double bi[4], x2[2];
-        inv2(r.be, bi);
-        mv2(bi, r.de, x2);
-        I.xi[3 * (size_t)k + 0] = x2[0];
-        I.xi[3 * (size_t)k + 1] = x2[1];
-        I.xi[3 * (size_t)k + 2] = b1[cur][k].de * rcp_or0(b1[cur][k].be);
+        const int g = k >> 5;
+        const double* o = reps + 13 * (size_t)k;
+        double xl[3] = {0.0, 0.0, 0.0};
+        if (g > 0)
+#pragma unroll
+            for (int t = 0; t < 3; ++t) xl[t] = X[3 * (g - 1) + t];
+        const double xr[3] = {X[3 * g], X[3 * g + 1], X[3 * g + 2]};
+        double x0 = o[0] + (o[3] * xl[0] + o[4] * xl[1]) + (o[8] * xr[0] + o[9] * xr[1]);
+        double x1 = o[1] + (o[5] * xl[0] + o[6] * xl[1]) + (o[10] * xr[0] + o[11] * xr[1]);
+        double x2 = o[2] + o[7] * xl[2] + o[12] * xr[2];
+        I.xi[3 * (size_t)k + 0] = x0;
+        I.xi[3 * (size_t)k + 1] = x1;
+        I.xi[3 * (size_t)k + 2] = x2;
     }
     __syncthreads();
 }
@@ -1341,11 +1470,10 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
 }
 
 constexpr size_t kSmemBytes = sizeof(WarpSmem) * kWarps;
-static_assert(2 * (sizeof(Red2) + sizeof(Red1)) * kMaxLoChunks <= kSmemBytes,
-              "reduced LO system must fit the CTA's shared memory");
-static_assert(sizeof(LoRow) * kMaxLoChunk + 13 * sizeof(double) * kMaxLoChunk <=
-                  sizeof(WarpSmem) - offsetof(WarpSmem, a),
-              "LO chunk scratch must fit a warp's shared memory");
+static_assert(sizeof(GroupRec) * (kMaxLoChunks / 32) + 13 * sizeof(double) * kMaxLoChunks +
+                      3 * sizeof(double) * (kMaxLoChunks / 32) <=
+                  kSmemBytes,
+              "interface system of the LO solve must fit the CTA's shared memory");
 
 }  // namespace holo
 }  // namespace keq
@@ -1384,10 +1512,8 @@ HDerived hderive(int nx, int nv, int kp) {
     d.rows = keq::kRmax;
     d.nchunks = (d.n_inner + d.rows - 1) / d.rows;
     d.nrb = (d.n_inner + keq::kRB - 1) / keq::kRB;
-    // LO chunks: multiples of 32 rows, few enough for the reduced system
-    int q = (d.n_inner + 32 * keq::holo::kMaxLoChunks - 1) / (32 * keq::holo::kMaxLoChunks);
-    if (q < 1) q = 1;
-    d.lo_len = 32 * q;
+    // LO chunks of 32 rows (one row per lane of the chunk's warp)
+    d.lo_len = keq::holo::kLoChunk;
     d.lo_k = (d.n_inner + d.lo_len - 1) / d.lo_len;
     return d;
 }
@@ -1561,7 +1687,7 @@ keq_status keq_holo_plan_create(const keq_instance* insts, int32_t n, const keq_
             }
         }
         const HDerived d = hderive(nx, nv, kp);
-        if (d.lo_len > holo::kMaxLoChunk || d.lo_k > holo::kMaxLoChunks) {
+        if (d.lo_k > holo::kMaxLoChunks) {
             delete plan;
             return KEQ_ERR_UNSUPPORTED;  // nx beyond the LO solver's capacity
         }
