@@ -515,6 +515,19 @@ __device__ __forceinline__ void warp_pcr(PcrRow& q, int L) {
         double Bi[4];
         inv2(q.B, Bi);
         const double bi = rcp_or0(q.b);
+        // Early exit once every row is decoupled to below double rounding:
+        // |B^{-1}|_inf (|A|_inf + |C|_inf) <= 2^-60 and the same for the
+        // scalar rows.  The couplings of an interface system are products of
+        // a chunk's 31 row couplings, so this usually holds before the first
+        // step there.  The test is warp-uniform and depends on the data only.
+        {
+            const double nbi = fmax(fabs(Bi[0]) + fabs(Bi[1]), fabs(Bi[2]) + fabs(Bi[3]));
+            const double nac = fmax(fabs(q.A[0]) + fabs(q.A[1]), fabs(q.A[2]) + fabs(q.A[3])) +
+                               fmax(fabs(q.C[0]) + fabs(q.C[1]), fabs(q.C[2]) + fabs(q.C[3]));
+            const double kTiny = 8.673617379884035e-19;  // 2^-60
+            const bool dec = nbi * nac <= kTiny && fabs(bi) * (fabs(q.a) + fabs(q.c)) <= kTiny;
+            if (__all_sync(0xffffffffu, dec || lane >= L)) break;
+        }
         const bool has_lo = lane >= d && lane < L, has_hi = lane + d < L;
         double nA[4], nC[4], dB[4], nR[10];
         double na, nc, db, nr[3];
