@@ -82,6 +82,7 @@ struct HoloInst {
     double* Wm;      // nx*3 : LO iterate W_m = (n, nu, U)
     double* Who;     // nx*3 : W_HO
     double* Iold;    // nx*3 : old collision moments (1-theta) C_old . w dv
+    double* Msum;    // nx*3 : velocity sums of M(f_z) per row: sum M, sum M v, sum M v^2 / 2
     double* Ib;      // 8    : boundary-row Maxwellian sums (2 rows x 3) + spare
     double* Y;       // nx*3 : consistency terms of the current HO iteration
     double* T1;      // nx*3 : W_HO - dt/2dx (F_HO diff) of the current HO iteration
@@ -289,27 +290,26 @@ __device__ __noinline__ void explicit_tile(WarpSmem& w, int vt, int c, const dou
     store_partials_h(w, g, vt);
 }
 
-// ---- A: Maxwellian partials of M(f_z) (one tile, no memory traffic) --------
-__device__ __noinline__ void maxwell_tile(WarpSmem& w, int vt, int c) {
+// ---- A: velocity sums of M(f_z) for one interior row (one warp) -----------
+// The Maxwellian of the row's moments (bgk1d_maxwellian.py:7-33) summed over
+// the velocity grid against 1, v and v^2/2, lane-strided with a fixed warp
+// reduction; lane 0 stores the three sums.
+__device__ __noinline__ void maxwell_row(WarpSmem& w, int k) {
     const HoloInst& I = w.I;
-    const int lane = threadIdx.x & 31;
-    const TileGeo g = inst_tile(I, vt, c, lane);
-    const double vj = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
-    w.vv[lane] = vj;
-    if (lane < g.nrows) {
-        const int i = scan_row(I.nx, g.pos, g.s0 + lane);
-        const Mom m = mom_of(I.R + 8 * (size_t)i, I.dv);
-        double c4[4];
-        mc_of(m, I.tau_tilde, c4);
-        w.coef[lane][0] = c4[0]; w.coef[lane][1] = c4[1]; w.coef[lane][2] = c4[2];
+    const int i = k + 1;
+    double R8[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) R8[q] = __ldcg(&I.R[8 * (size_t)i + q]);
+    const Mom m = mom_of(R8, I.dv);
+    double c4[4];
+    mc_of(m, I.tau_tilde, c4);
+    double s3[3];
+    maxwell_sums_row(I.v, I.nv, c4, s3);
+    if ((threadIdx.x & 31) == 0) {
+        I.Msum[3 * (size_t)i + 0] = s3[0];
+        I.Msum[3 * (size_t)i + 1] = s3[1];
+        I.Msum[3 * (size_t)i + 2] = s3[2];
     }
-    __syncwarp();
-    for (int r = 0; r < g.nrows; ++r) {
-        const double d = vj - w.coef[r][0];
-        const double M = w.coef[r][2] * exp_nonpos(d * d * w.coef[r][1]);
-        w.a[r][lane] = g.lane_ok ? M : 0.0;
-    }
-    store_partials_h(w, g, vt);
 }
 
 // ---- LO: structured blocks -----------------------------------------------------
@@ -451,11 +451,11 @@ __device__ __noinline__ double lo_prep_row(const HoloInst& I, int k) {
             for (int c = 0; c < 3; ++c) y[c] = dt * ((g[1][c] - g[0][c]) / dx);
         }
         // collision consistency: theta C_new + (1-theta) C_old moments
-        double sM[4];
-        sum_partials4(I.part, 0, I.nvt, I.n_inner, k, sM);
         const Mom& mn = m3[1];
         const double inv_tau_new = (mn.n * sqrt(mn.T)) / I.tau_tilde;
-        const double smw[3] = {sM[0] * dv, sM[1] * dv, 0.5 * (sM[2] * dv)};
+        const double smw[3] = {__ldcg(&I.Msum[3 * (size_t)i]) * dv,
+                               __ldcg(&I.Msum[3 * (size_t)i + 1]) * dv,
+                               __ldcg(&I.Msum[3 * (size_t)i + 2]) * dv};
         const double sfw[3] = {mn.n, mn.s1, 0.5 * mn.s2};
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -1294,19 +1294,28 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
         if (!any) break;
 
         trace_h(P, z, 0, true);
-        // A: Maxwellian partials of M(f_z); W_m = W_HO; boundary |Y| into max_YI
-        for (long long t = gwarp; t < total_tiles; t += nwarps) {
-            const int b = find_inst(P.tile_off, n_inst, t);
+        // A: velocity sums of M(f_z) per interior row (one warp per row);
+        // W_m = W_HO; boundary |Y| into max_YI
+        for (long long u = gwarp; u < total_rb * kRB; u += nwarps) {
+            const long long rb = u / kRB;
+            const int b = find_inst(P.rb_off, n_inst, rb);
             stage_warp(w, &P.inst[b], b);
             if (!ho_active(w.I, z) || !w.I.con_terms) continue;
-            const long long tl = t - w.I.tile_off;
-            maxwell_tile(w, (int)(tl % w.I.nvt), (int)(tl / w.I.nvt));
+            const int k = (int)(rb - w.I.rb_off) * kRB + (int)(u % kRB);
+            if (k < w.I.n_inner) maxwell_row(w, k);
         }
-        for (int b = blockIdx.x; b < n_inst; b += G) {
-            const HoloInst& I = P.inst[b];
-            if (!ho_active(I, z)) continue;
-            for (int q = threadIdx.x; q < 3 * I.nx; q += kThreads) I.Wm[q] = __ldcg(&I.Who[q]);
-            if (threadIdx.x == 0) atomic_max_nonneg(&I.ho_red[4 * z + 3], __ldcg(&I.misc[1]));
+        // W_m = W_HO, spread over every thread of the grid (one element each
+        // for a 4096-row instance; a single CTA would take ~100 dependent
+        // load-store rounds)
+        {
+            const long long gt = (long long)blockIdx.x * kThreads + threadIdx.x;
+            const long long gn = (long long)G * kThreads;
+            for (int b = 0; b < n_inst; ++b) {
+                const HoloInst& I = P.inst[b];
+                if (!ho_active(I, z)) continue;
+                for (long long q = gt; q < 3LL * I.nx; q += gn) I.Wm[q] = __ldcg(&I.Who[q]);
+                if (gt == 0) atomic_max_nonneg(&I.ho_red[4 * z + 3], __ldcg(&I.misc[1]));
+            }
         }
         trace_h(P, z, 1, false);
         if (!holo_sync(P, G)) return;
@@ -1550,6 +1559,7 @@ size_t carve_holo(void* base, int nx, int nv, int kp, const keq_holo_params& p, 
     double* Wm = c.take<double>(3 * (size_t)nx);
     double* Who = c.take<double>(3 * (size_t)nx);
     double* Iold = c.take<double>(3 * (size_t)nx);
+    double* Msum = c.take<double>(3 * (size_t)nx);
     double* Ib = c.take<double>(8);
     double* Y = c.take<double>(3 * (size_t)nx);
     double* T1 = c.take<double>(3 * (size_t)nx);
@@ -1568,7 +1578,7 @@ size_t carve_holo(void* base, int nx, int nv, int kp, const keq_holo_params& p, 
     double* misc = c.take<double>(8);
     if (I) {
         I->E = E; I->part = part; I->R = R; I->Rn = Rn; I->Mco = Mco; I->Wm = Wm; I->Who = Who;
-        I->Iold = Iold; I->Ib = Ib; I->Y = Y; I->T1 = T1; I->lorow = lorow; I->loedge = loedge;
+        I->Iold = Iold; I->Msum = Msum; I->Ib = Ib; I->Y = Y; I->T1 = T1; I->lorow = lorow; I->loedge = loedge;
         I->xi = xi; I->Wlo = Wlo; I->agg = agg; I->inc = inc; I->flag = flag; I->rbcnt = rbcnt;
         I->ho_red = ho_red; I->lo_hist = lo_hist; I->ho_run = ho_run; I->lo_run = lo_run;
         I->nonfin = nonfin; I->misc = misc;
