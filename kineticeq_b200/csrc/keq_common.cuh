@@ -146,6 +146,19 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// Number of leading entries equal to 1 in flags[0..n) (the iterations that
+// ran), by a whole warp: 32 flags per load round, first miss by ballot.
+__device__ __forceinline__ int count_leading_ones(const int* flags, int n) {
+    const int lane = threadIdx.x & 31;
+    for (int base = 0; base < n; base += 32) {
+        const int q = base + lane;
+        const bool miss = q >= n || __ldcg(&flags[q]) != 1;
+        const unsigned mm = __ballot_sync(0xffffffffu, miss);
+        if (mm != 0u) return base + __ffs(mm) - 1 < n ? base + __ffs(mm) - 1 : n;
+    }
+    return n;
+}
+
 __device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = nan_max(v, __shfl_xor_sync(0xffffffffu, v, o));

@@ -1289,9 +1289,11 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
     if (!holo_sync(P, G)) return;
 
     for (int z = 0; z < P.max_ho; ++z) {
-        bool any = false;
-        for (int b = 0; b < n_inst && !any; ++b) any = ho_active(P.inst[b], z);
-        if (!any) break;
+        // any instance active in HO iteration z (a share of the instances per
+        // thread, combined over the CTA)
+        bool mine = false;
+        for (int b = threadIdx.x; b < n_inst && !mine; b += kThreads) mine = ho_active(P.inst[b], z);
+        if (!__syncthreads_or(mine)) break;
 
         trace_h(P, z, 0, true);
         // A: velocity sums of M(f_z) per interior row (one warp per row);
@@ -1323,9 +1325,10 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
         trace_h(P, z, 2, true);
         // LO Picard iterations
         for (int m = 0; m < P.max_lo; ++m) {
-            bool lany = false;
-            for (int b = 0; b < n_inst && !lany; ++b) lany = lo_active(P.inst[b], z, m);
-            if (!lany) break;
+            bool lmine = false;
+            for (int b = threadIdx.x; b < n_inst && !lmine; b += kThreads)
+                lmine = lo_active(P.inst[b], z, m);
+            if (!__syncthreads_or(lmine)) break;
             if (m == 0) trace_h(P, z, 8, true);
             // L1
             for (long long u = gwarp; u < total_lo; u += nwarps) {
@@ -1450,22 +1453,16 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
     // E: statistics (benchlog keys of :586-594)
     if (blockIdx.x == 0 && threadIdx.x == 0) P.head.fresh = 0;
     for (int b = blockIdx.x; b < n_inst; b += G) {
-        if (threadIdx.x != 0) continue;
+        if (threadIdx.x >= 32) continue;
         const HoloInst& I = P.inst[b];
-        int last = -1;
-        for (int z = 0; z < I.ho_iter; ++z) {
-            if (__ldcg(&I.ho_run[z]) == 1) last = z;
-            else break;
-        }
+        const int last = count_leading_ones(I.ho_run, I.ho_iter) - 1;
+        const int lo_last =
+            last >= 0 ? count_leading_ones(I.lo_run + (size_t)last * I.lo_iter, I.lo_iter) - 1 : -1;
+        if (threadIdx.x != 0) continue;
         keq_step_stats* st = I.stats;
         int status = KEQ_OK;
-        int lo_last = -1;
         double lo_df = 0.0, lo_std = 0.0, ho_std = 0.0, ho_rel = 0.0, myi = 0.0;
         if (last >= 0) {
-            for (int m = 0; m < I.lo_iter; ++m) {
-                if (__ldcg(&I.lo_run[(size_t)last * I.lo_iter + m]) == 1) lo_last = m;
-                else break;
-            }
             if (lo_last >= 0) {
                 lo_df = __ldcg(&I.lo_hist[2 * ((size_t)last * I.lo_iter + lo_last)]);
                 lo_std = __ldcg(&I.lo_hist[2 * ((size_t)last * I.lo_iter + lo_last) + 1]);

@@ -983,9 +983,11 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
 
     // Picard iterations
     for (int m = 0; m < P.max_iter; ++m) {
-        bool any = false;
-        for (int b = 0; b < n_inst && !any; ++b) any = inst_active(P.inst[b], m);
-        if (!any) break;
+        // any instance active in iteration m: every thread tests a share of
+        // the instances, combined over the CTA (the same answer in every CTA)
+        bool mine = false;
+        for (int b = threadIdx.x; b < n_inst && !mine; b += kThreads) mine = inst_active(P.inst[b], m);
+        if (!__syncthreads_or(mine)) break;
         const unsigned long long epoch = seq * (unsigned long long)(P.max_iter + 1) + m + 1;
 
         trace_mark(P, m, 0, true);
@@ -1038,14 +1040,11 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
     // E: statistics
     if (blockIdx.x == 0 && threadIdx.x == 0) P.head.fresh = 0;
     for (int b = blockIdx.x; b < n_inst; b += G) {
-        if (threadIdx.x != 0) continue;
+        if (threadIdx.x >= 32) continue;
         const ImpInst& I = P.inst[b];
         if (!inst_enabled(I)) continue;
-        int last = -1;
-        for (int m = 0; m < I.picard_iter; ++m) {
-            if (__ldcg(&I.st[m]) == 1) last = m;
-            else break;
-        }
+        const int last = count_leading_ones(I.st, I.picard_iter) - 1;
+        if (threadIdx.x != 0) continue;
         keq_step_stats* s = I.stats;
         int aa_applied = 0;
         for (int m = 0; m < last; ++m)
