@@ -404,10 +404,12 @@ def run_reference(args, dist, rank, world):
 # distribution, 100..2000 steps per request).
 # ---------------------------------------------------------------------------
 MIX_WORKLOADS = {
-    # name: (kind, instances, seed, rate per s)
-    "batch-cfg3-256": ("batch", 256, 0, None),
-    "serve-cfg5-r200": ("serve", 64, 0, 200.0),
-    "serve-cfg5-r50": ("serve", 32, 1, 50.0),
+    # name: (kind, instances, seed, rate per s, precision of the solves)
+    "batch-cfg3-256": ("batch", 256, 0, None, "fp64"),
+    "batch-cfg3-256-mixed": ("batch", 256, 0, None, "mixed"),
+    "serve-cfg5-r200": ("serve", 64, 0, 200.0, "fp64"),
+    "serve-cfg5-r200-mixed": ("serve", 64, 0, 200.0, "mixed"),
+    "serve-cfg5-r50": ("serve", 32, 1, 50.0, "fp64"),
 }
 MIX_PARAMS = dict(picard_iter=64, picard_tol=1e-10, abs_tol=1e-16)
 
@@ -464,16 +466,20 @@ def run_mix(args, dist, rank, world):
     from kineticeq_b200.batch import BatchSolver, sample_instances
     from kineticeq_b200.serving import Server, plain_throughput, poisson_stream
 
-    kind, n_inst, seed, rate = MIX_WORKLOADS[args.workload]
+    kind, n_inst, seed, rate, prec = MIX_WORKLOADS[args.workload]
+    # our solves run in `prec`; the plain comparison and the CPU baseline are
+    # always the reference's FP64 method
+    params = dict(MIX_PARAMS, precision=prec) if prec != "fp64" else MIX_PARAMS
     table = autotune.load() or {}
     out = {"metric": METRIC, "unit": METRIC, "n_gpus": world, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64" if prec == "fp64" else "f32 sweeps then f64 sweeps (mixed)",
            "data": "synthetic (seeded two-state Riemann instances, sizes and states as the "
                    "batching distribution)"}
     launches = 0
     if kind == "batch":
         descs = sample_instances(n_inst, seed=seed + rank)
-        solver = BatchSolver(descs, MIX_PARAMS, table=table)
+        solver = BatchSolver(descs, params, table=table)
         cells = solver.cells
         for _ in range(args.warmup):
             solver.step(1)
@@ -533,7 +539,7 @@ def run_mix(args, dist, rank, world):
                     "ms_per_step": round(ms / args.steps, 4),
                     "plain_value": round(plain, 1), "speedup_vs_plain": round(value / plain, 3),
                     "config": {"workload": args.workload, "instances": n_inst, "seed": seed,
-                               "cells_per_step": cells, "dt": 5e-6, **MIX_PARAMS,
+                               "cells_per_step": cells, "dt": 5e-6, **params,
                                "tile_rows_table": bool(table), "cuda_graph": use_graph,
                                "l2": "inputs larger than L2 (535 MB per FP64 field)",
                                "mean_picard_iters_per_step":
@@ -548,10 +554,10 @@ def run_mix(args, dist, rank, world):
     else:
         reqs = poisson_stream(n_inst, rate, seed=seed + rank)
         warm = poisson_stream(4, 1e6, seed=99, steps_range=(3, 3))
-        Server(params=MIX_PARAMS, table=table).run(warm, realtime=False)
+        Server(params=params, table=table).run(warm, realtime=False)
         _barrier(dist)
         with ClockSampler(torch.cuda.current_device()) as clk:
-            res = Server(params=MIX_PARAMS, table=table).run(reqs)
+            res = Server(params=params, table=table).run(reqs)
         _barrier(dist)
         ms = _max_over_ranks(dist, res["makespan_s"] * 1e3)
         launches = res["launches"]
@@ -567,7 +573,7 @@ def run_mix(args, dist, rank, world):
             for r in reqs2:
                 r.f0_host = make_state(r.desc).f.cpu().pin_memory()
             torch.cuda.synchronize()
-            res2 = Server(params=MIX_PARAMS, table=table, copy_out=True).run(reqs2)
+            res2 = Server(params=params, table=table, copy_out=True).run(reqs2)
             nb = sum(8 * r.desc.cells for r in reqs2)
             e2e = {"value": round(world * res2["cell_steps"] / res2["makespan_s"], 1),
                    "unit": METRIC, "h2d_bytes_per_step": round(nb / res2["steps"]),
@@ -583,7 +589,7 @@ def run_mix(args, dist, rank, world):
                     "plain_value": round(plain, 1), "speedup_vs_plain": round(value / plain, 3),
                     "config": {"workload": args.workload, "requests": n_inst, "rate_per_s": rate,
                                "seed": seed, "steps_per_request": "uniform 100..2000",
-                               **MIX_PARAMS, "rebuilds": res["rebuilds"],
+                               **params, "rebuilds": res["rebuilds"],
                                "l2": "inputs larger than L2 in aggregate; not flushed",
                                "plain": plain_sample},
                     "clocks": clk.summary()})
@@ -602,7 +608,7 @@ def run_mix_reference(args, dist, rank, world):
         return
     from kineticeq_b200.batch import sample_instances
 
-    kind, n_inst, seed, rate = MIX_WORKLOADS[args.workload]
+    kind, n_inst, seed, rate, _prec = MIX_WORKLOADS[args.workload]
     descs = sample_instances(n_inst, seed=seed,
                              steps_range=None if kind == "batch" else (100, 2000))
     v, sample = _oracle_rate(descs, MIX_PARAMS, args.cpu_seconds * 6)

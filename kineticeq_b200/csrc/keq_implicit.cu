@@ -217,18 +217,45 @@ __device__ __forceinline__ void stage_warp(WarpSmem& w, const ImpInst* src, int 
     __syncwarp();
 }
 
-// Activity of the staged instance in iteration m, cached per warp.
+// Warp-collective fp32_iter (every lane with the same I and m): the earlier
+// residuals are read 32 per round instead of one dependent load at a time.
+__device__ __forceinline__ bool fp32_iter_warp(const ImpInst& I, int m) {
+    if (!I.mixed || I.fixed_iters > 0 || m >= I.picard_iter / 2) return false;
+    const int lane = threadIdx.x & 31;
+    for (int base = 0; base < m; base += 32) {
+        const int k = base + lane;
+        const bool met = k < m && ld_cg(&I.res[2 * k]) <= 1.0;
+        if (__any_sync(0xffffffffu, met)) return false;
+    }
+    return true;
+}
+
+// inst_active with fp32_iter(I, m-1) already known.
+__device__ __forceinline__ bool inst_active_known(const ImpInst& I, int m, bool prev32) {
+    if (m >= I.picard_iter || !inst_enabled(I)) return false;
+    if (m == 0) return true;
+    if (__ldcg(&I.st[m - 1]) != 1) return false;
+    if (I.fixed_iters > 0) return m < I.fixed_iters;
+    if (prev32) return true;
+    return !(ld_cg(&I.res[2 * (m - 1)]) <= 1.0);
+}
+
+// Activity of the staged instance in iteration m and whether iterations m
+// and m-1 are FP32 sweeps, cached per warp (bit 0 active, bit 1 iteration m
+// is an FP32 sweep, bit 2 iteration m-1 was).  Warp-collective.
 __device__ __forceinline__ bool staged_active(WarpSmem& w, int m) {
     if (w.cur_m != m) {
-        const bool a = inst_active(w.I, m);
+        const bool p32 = m > 0 && fp32_iter_warp(w.I, m - 1);
+        const bool a = inst_active_known(w.I, m, p32);
+        const bool c32 = a && fp32_iter_warp(w.I, m);
         __syncwarp();
         if ((threadIdx.x & 31) == 0) {
-            w.cur_active = a ? 1 : 0;
+            w.cur_active = (a ? 1 : 0) | (c32 ? 2 : 0) | (p32 ? 4 : 0);
             w.cur_m = m;
         }
         __syncwarp();
     }
-    return w.cur_active != 0;
+    return (w.cur_active & 1) != 0;
 }
 
 // Asynchronous copy of a tile's rows into shared memory (one 8-byte element
@@ -355,7 +382,7 @@ __device__ bool picard_tile(WarpSmem& w, int vt, int c, int m, unsigned long lon
     // at m = 0; the FP32 iterate after the FP32 sweeps of the mixed form) is
     // streamed into registers 8 rows ahead of the recurrence, the first 8
     // rows before the look-back
-    const bool ref32 = m > 0 && fp32_iter(I, m - 1);
+    const bool ref32 = (w.cur_active & 4) != 0;  // iteration m-1 was an FP32 sweep
     const double* ref64 = m > 0 ? fo : fn;
     stage_rows<33>(w.a, fn, g, nx, nv);
     cp_async_commit();
@@ -1006,7 +1033,7 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
             const int c = (int)(tl / w.I.nvt), vt = (int)(tl % w.I.nvt);
             const double* fn = swap_io ? w.I.f_out : w.I.f_in;
             double* fo = swap_io ? const_cast<double*>(w.I.f_in) : w.I.f_out;
-            const bool is32 = fp32_iter(w.I, m);
+            const bool is32 = (w.cur_active & 2) != 0;  // staged_active above
             const bool ok = is32 ? picard_tile32(w, vt, c, m, epoch, limit, fn, q1, q2, bad)
                                  : picard_tile(w, vt, c, m, epoch, limit, fn, fo, q1, q2, bad);
             if (!ok) {
