@@ -55,6 +55,11 @@ WORKLOADS = {
                                             aa_enable=True, aa_m=5), 200),
     "implicit-8192x1024-tau1e-4": (8192, 1024, 1e-5, 1e-4,
                                    dict(picard_iter=64, picard_tol=1e-10, abs_tol=1e-16), 200),
+    # the precision form: FP32 sweeps then FP64 sweeps; the bench line adds the
+    # error in rho, u, T against the FP64 method over the same steps
+    "implicit-8192x1024-tau1e-4-mixed": (8192, 1024, 1e-5, 1e-4,
+                                         dict(picard_iter=64, picard_tol=1e-10, abs_tol=1e-16,
+                                              precision="mixed"), 200),
     "holo-4096x512-tau5e-5": (4096, 512, 1e-5, 5e-5,
                               dict(scheme="holo", ho_iter=64, ho_tol=1e-10, lo_iter=64,
                                    lo_tol=1e-10), 200),
@@ -249,6 +254,8 @@ def run_ours(args, dist, rank, world):
     if int(rec["status"]) != 0:
         raise RuntimeError(f"device status {N.status_text(int(rec['status']))}")
     iters = int(rec["total_iters"]) - iters0
+    prec_err = _precision_error(name, plan.state(0), f0, st, args.steps) \
+        if sp.get("precision") == "mixed" else None
     # conservation drift over the timed steps (row moments on the device)
     from kineticeq_b200.schemes.common import conservation_totals, drift
 
@@ -304,6 +311,8 @@ def run_ours(args, dist, rank, world):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 5),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (Sod initial state, generated on the device)",
+            **({"dtype": "f32 sweeps then f64 sweeps (mixed)", "precision_error": prec_err}
+               if prec_err is not None else {}),
             "config": {"workload": name, "scheme": "holo" if holo else "implicit", "nx": nx,
                        "nv": nv, "dt": dt, "tau_tilde": tau, **sp,
                        "instances_per_gpu": 1, "parallelism": f"replicas x{world}",
@@ -316,6 +325,37 @@ def run_ours(args, dist, rank, world):
             "clocks": clk.summary(),
         }
         print(json.dumps(out))
+
+
+def _precision_error(name, f_mixed, f0, st, steps):
+    """Relative max error of the mixed-precision result against the FP64
+    method run from the same initial state for the same steps: f normwise and
+    the row moments rho, u, T (max |d| / max |ref|)."""
+    import torch
+
+    from kineticeq_b200.plan import ImplicitPlan, InstanceSpec, implicit_params_struct
+
+    nx, nv, dt, tau, _, _ = WORKLOADS[name]
+    sp = dict(scheme_params(name), precision="fp64")
+    a = f0.clone()
+    spec = InstanceSpec(v=st.v, dx=st.dx, dv=st.dv, dt=dt, tau_tilde=tau, a=a,
+                        b=torch.empty_like(a))
+    ref_plan = ImplicitPlan([spec], implicit_params_struct(**sp))
+    ref_plan.step(steps)
+    ref = ref_plan.state(0)
+
+    def mom(f):
+        n = f.sum(1) * st.dv
+        u = (f * st.v).sum(1) * st.dv / n
+        T = (f * st.v * st.v).sum(1) * st.dv / n - u * u
+        return n, u, T
+
+    def rel(x, y):
+        return float((x - y).abs().max() / y.abs().max().clamp_min(1e-300))
+
+    (n1, u1, T1), (n0, u0, T0) = mom(f_mixed), mom(ref)
+    return {"f": rel(f_mixed, ref), "rho": rel(n1, n0), "u": rel(u1, u0), "T": rel(T1, T0),
+            "against": f"FP64 method, same {steps} steps from the same state"}
 
 
 def cpu_baseline(name, f0, st, budget_s=20.0):
