@@ -210,9 +210,9 @@ void keq_plan_destroy(keq_plan* plan);
  * with the keq_plan_* functions above.  Each step fills the instance's
  * keq_step_stats with iters = ho_iter, residual = ho_residual, std_residual =
  * std_ho_residual, lo_iters, lo_residual, std_lo_residual and max_YI (the
- * reference's benchlog).  Supported sizes: nx - 2 <= 15872 interior cells
- * (the LO interface system is solved in one CTA's shared memory); larger
- * grids return KEQ_ERR_UNSUPPORTED. */
+ * reference's benchlog).  Supported sizes: nx - 2 <= 16384 interior cells
+ * (512 LO chunks of 32 rows; the interface system is solved in one CTA's
+ * shared memory); larger grids return KEQ_ERR_UNSUPPORTED. */
 keq_status keq_holo_instance_workspace_size(const keq_grid* grid, const keq_holo_params* params,
                                             size_t* bytes);
 keq_status keq_holo_plan_workspace_size(const keq_instance* insts, int32_t n,
