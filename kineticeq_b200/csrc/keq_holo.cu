@@ -86,7 +86,8 @@ struct HoloInst {
     double* Ib;      // 8    : boundary-row Maxwellian sums (2 rows x 3) + spare
     double* Y;       // nx*3 : consistency terms of the current HO iteration
     double* T1;      // nx*3 : W_HO - dt/2dx (F_HO diff) of the current HO iteration
-    double* lorow;   // n_inner*13 : y(3) | P(2x2) | P_U | Q(2x2) | Q_U per row
+    double* lorow;   // 2*n_inner*13 : y(3) | P(2x2) | P_U | Q(2x2) | Q_U per row, one set per
+                     // LO-iteration parity (iteration m writes set m & 1)
     double* loedge;  // lo_k*18 : last-row blocks of each chunk (A,B,C 2x2, D 2 | U: a,b,c,d)
     double* xi;      // lo_k*3 : interface unknowns
     double* Wlo;     // 3*nx : n_lo | u_lo | T_lo of the last LO solve (state.n/u/T)
@@ -351,13 +352,13 @@ __device__ __forceinline__ double rcp_or0(double d) { return fabs(d) >= 1e-30 ? 
 // Block row of interior row k (cell i = k+1) from W_m: faces L (i-1, i) and
 // R (i, i+1); AA = -c4 A_L (0 at k = 0), CC = c4 A_R (0 at the last row),
 // BB = I + c4 (A_R - A_L), DD = ((T1 - c2 (b_R - b_L)) + Y).
-__device__ __forceinline__ void lo_row(const HoloInst& I, int k, LoRow& r) {
+__device__ __forceinline__ void lo_row_w(const HoloInst& I, int k, const double* Wl,
+                                         const double* Wc, const double* Wr, LoRow& r) {
     const int i = k + 1;
-    const double* W = I.Wm;
     double uL, PL, uC, PC, uR, PR;
-    star_of(W + 3 * (size_t)(i - 1), uL, PL);
-    star_of(W + 3 * (size_t)i, uC, PC);
-    star_of(W + 3 * (size_t)(i + 1), uR, PR);
+    star_of(Wl, uL, PL);
+    star_of(Wc, uC, PC);
+    star_of(Wr, uR, PR);
     const double uhL = 0.5 * (uL + uC), PhL = 0.5 * (PL + PC);
     const double uhR = 0.5 * (uC + uR), PhR = 0.5 * (PC + PR);
     const double c4 = I.dt / (4.0 * I.dx), c2 = I.dt / (2.0 * I.dx);
@@ -380,6 +381,13 @@ __device__ __forceinline__ void lo_row(const HoloInst& I, int k, LoRow& r) {
     r.D[0] = __dadd_rn(__dadd_rn(__ldcg(&T1[0]), __dmul_rn(-c2, bd0)), __ldcg(&Y[0]));
     r.D[1] = __dadd_rn(__dadd_rn(__ldcg(&T1[1]), __dmul_rn(-c2, bd1)), __ldcg(&Y[1]));
     r.d = __dadd_rn(__dadd_rn(__ldcg(&T1[2]), __dmul_rn(-c2, bd2)), __ldcg(&Y[2]));
+}
+
+// The same from the LO iterate in I.Wm (rows i-1, i, i+1).
+__device__ __forceinline__ void lo_row(const HoloInst& I, int k, LoRow& r) {
+    const int i = k + 1;
+    lo_row_w(I, k, I.Wm + 3 * (size_t)(i - 1), I.Wm + 3 * (size_t)i, I.Wm + 3 * (size_t)(i + 1),
+             r);
 }
 
 // Constant part of the LO right-hand side and the consistency terms Y of row
@@ -659,15 +667,13 @@ __device__ __forceinline__ void local_rows(PcrRow& q, const double* A, const dou
 // interface row), the warp-parallel solve of the local rows s..e-1 into the
 // representation x_r = y_r + P_r xi_{k-1} + Q_r xi_k (row e: y = 0, P = 0,
 // Q = I) in lorow, and the interface row's blocks in loedge.
-__device__ __noinline__ void lo_chunk_eliminate(WarpSmem& w, int kc) {
-    const HoloInst& I = w.I;
+__device__ __forceinline__ void lo_chunk_solve(const HoloInst& I, int kc, const LoRow& L,
+                                               double* __restrict__ lorow) {
     const int lane = threadIdx.x & 31;
     const int s = kc * I.lo_len;
     const int e = (s + I.lo_len < I.n_inner ? s + I.lo_len : I.n_inner) - 1;
     const int len = e - s + 1;
     const int nloc = len - 1;  // rows s..e-1 solved locally
-    LoRow L{};
-    if (lane < len) lo_row(I, s + lane, L);
     if (lane == nloc) {
         double* ed = I.loedge + (size_t)kc * 18;
 #pragma unroll
@@ -691,10 +697,22 @@ __device__ __noinline__ void lo_chunk_eliminate(WarpSmem& w, int kc) {
             for (int k = 0; k < 13; ++k) o[k] = 0.0;
             o[8] = 1.0; o[11] = 1.0; o[12] = 1.0;
         }
-        double* dst = I.lorow + 13 * (size_t)(s + lane);
+        double* dst = lorow + 13 * (size_t)(s + lane);
 #pragma unroll
         for (int k = 0; k < 13; ++k) dst[k] = o[k];
     }
+}
+
+// L1 of the first LO iteration: block rows from W_m = W_HO in I.Wm, solved
+// into the representation set `lorow`.
+__device__ __noinline__ void lo_chunk_eliminate(WarpSmem& w, int kc, double* __restrict__ lorow) {
+    const HoloInst& I = w.I;
+    const int lane = threadIdx.x & 31;
+    const int s = kc * I.lo_len;
+    const int e = (s + I.lo_len < I.n_inner ? s + I.lo_len : I.n_inner) - 1;
+    LoRow L{};
+    if (lane <= e - s) lo_row(I, s + lane, L);
+    lo_chunk_solve(I, kc, L, lorow);
 }
 
 // Representation (y, P, Q) of a row: from lorow, or the identity forms
@@ -709,8 +727,9 @@ __device__ __forceinline__ void rep_load(const double* lr, double* o13) {
 //   alpha = A_e P_{e-1}, beta = B_e + A_e Q_{e-1} + C_e P_{s'},
 //   gamma = C_e Q_{s'}, delta = D_e - A_e y_{e-1} - C_e y_{s'}
 // (s' the first row of chunk k+1), the same for the U scalar.
-__device__ __forceinline__ void interface_row(const HoloInst& I, int k, double* al, double* be,
-                                              double* ga, double* de, double* s4) {
+__device__ __forceinline__ void interface_row(const HoloInst& I, const double* lorow, int k,
+                                              double* al, double* be, double* ga, double* de,
+                                              double* s4) {
     const int s = k * I.lo_len;
     const int e = (s + I.lo_len < I.n_inner ? s + I.lo_len : I.n_inner) - 1;
     double ed[18];
@@ -720,14 +739,14 @@ __device__ __forceinline__ void interface_row(const HoloInst& I, int k, double* 
     const double* D = ed + 12;
     double pm[13], nx_[13];
     if (e > s) {
-        rep_load(I.lorow + 13 * (size_t)(e - 1), pm);
+        rep_load(lorow + 13 * (size_t)(e - 1), pm);
     } else {
 #pragma unroll
         for (int q = 0; q < 13; ++q) pm[q] = 0.0;
         pm[3] = 1.0; pm[6] = 1.0; pm[7] = 1.0;
     }
     if (k + 1 < I.lo_k) {
-        rep_load(I.lorow + 13 * (size_t)(e + 1), nx_);
+        rep_load(lorow + 13 * (size_t)(e + 1), nx_);
     } else {
 #pragma unroll
         for (int q = 0; q < 13; ++q) nx_[q] = 0.0;
@@ -762,7 +781,8 @@ struct GroupRec {
     double al[4], be[4], ga[4], de[2], s4[4];  // the group's last interface row
 };
 
-__device__ __noinline__ void lo_reduced_solve(const HoloInst& I, unsigned char* smem) {
+__device__ __noinline__ void lo_reduced_solve(const HoloInst& I, const double* lorow,
+                                              unsigned char* smem) {
     const int K = I.lo_k;
     const int G = (K + 31) / 32;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -776,7 +796,7 @@ __device__ __noinline__ void lo_reduced_solve(const HoloInst& I, unsigned char* 
         const int k = k0 + lane;
         double al[4] = {0, 0, 0, 0}, be[4] = {1, 0, 0, 1}, ga[4] = {0, 0, 0, 0}, de[2] = {0, 0};
         double s4[4] = {0.0, 1.0, 0.0, 0.0};
-        if (lane < len) interface_row(I, k, al, be, ga, de, s4);
+        if (lane < len) interface_row(I, lorow, k, al, be, ga, de, s4);
         PcrRow q;
         local_rows(q, al, be, ga, de, s4[0], s4[1], s4[2], s4[3], lane, nloc);
         warp_pcr(q, nloc);
@@ -881,27 +901,49 @@ __device__ __noinline__ void lo_reduced_solve(const HoloInst& I, unsigned char* 
     __syncthreads();
 }
 
-// L3: recovery of chunk kc's rows, W_full, the LO residual (max |dW| and
-// max |dW| / (abs + tol max(|W_full|, |W_m|))) and W_m <- W_full.
-__device__ __noinline__ void lo_chunk_recover(WarpSmem& w, int kc, int z, int m) {
+// x = y + P xl + Q xr for a row with representation o (13 values), in one
+// fixed, non-contracted order: a chunk's warp recovers its rows with it, and
+// the previous chunk's warp recomputes this chunk's first row with it, so
+// both get the same value.
+__device__ __forceinline__ void rep_apply(const double* o, const double* xl, const double* xr,
+                                          double* x) {
+    x[0] = __dadd_rn(__dadd_rn(o[0], __dadd_rn(__dmul_rn(o[3], xl[0]), __dmul_rn(o[4], xl[1]))),
+                     __dadd_rn(__dmul_rn(o[8], xr[0]), __dmul_rn(o[9], xr[1])));
+    x[1] = __dadd_rn(__dadd_rn(o[1], __dadd_rn(__dmul_rn(o[5], xl[0]), __dmul_rn(o[6], xl[1]))),
+                     __dadd_rn(__dmul_rn(o[10], xr[0]), __dmul_rn(o[11], xr[1])));
+    x[2] = __dadd_rn(__dadd_rn(o[2], __dmul_rn(o[7], xl[2])), __dmul_rn(o[12], xr[2]));
+}
+
+// L3 of LO iteration m fused with L1 of iteration m+1, by the chunk's warp
+// (lane = row): recovery of the rows from the representation set `cur` and
+// the interface values (W_full, the LO residual, W_m <- W_full); then, when
+// `next` is given, the block rows of iteration m+1 from the recovered values
+// and their solve into the set `next`.  The neighbours outside the chunk are
+// the previous chunk's interface value (row s-1), the next chunk's first row
+// recomputed from its representation in `cur` (row e+1), or the fixed
+// boundary cells, so no barrier is needed between the two halves.  Iteration
+// m+1 is prepared before it is known whether iteration m converged; if it
+// did, the prepared rows are not used.
+__device__ __noinline__ void lo_chunk_step(WarpSmem& w, int kc, int z, int m,
+                                           const double* __restrict__ cur,
+                                           double* __restrict__ next) {
     const HoloInst& I = w.I;
     const int lane = threadIdx.x & 31;
     const int s = kc * I.lo_len;
     const int e = (s + I.lo_len < I.n_inner ? s + I.lo_len : I.n_inner) - 1;
+    const int len = e - s + 1;
     double xl[3] = {0.0, 0.0, 0.0}, xr[3];
     if (kc > 0)
         for (int q = 0; q < 3; ++q) xl[q] = __ldcg(&I.xi[3 * (size_t)(kc - 1) + q]);
     for (int q = 0; q < 3; ++q) xr[q] = __ldcg(&I.xi[3 * (size_t)kc + q]);
+    double x[3] = {0.0, 0.0, 0.0};
     double mdf = 0.0;
     FracMax fm;
-    for (int r = s + lane; r <= e; r += 32) {
-        const double* o = I.lorow + 13 * (size_t)r;
+    const int r = s + lane;
+    if (lane < len) {
         double o13[13];
-        rep_load(o, o13);
-        double x[3];
-        x[0] = o13[0] + (o13[3] * xl[0] + o13[4] * xl[1]) + (o13[8] * xr[0] + o13[9] * xr[1]);
-        x[1] = o13[1] + (o13[5] * xl[0] + o13[6] * xl[1]) + (o13[10] * xr[0] + o13[11] * xr[1]);
-        x[2] = o13[2] + o13[7] * xl[2] + o13[12] * xr[2];
+        rep_load(cur + 13 * (size_t)r, o13);
+        rep_apply(o13, xl, xr, x);
         if (r == e) { x[0] = xr[0]; x[1] = xr[1]; x[2] = xr[2]; }
         double* Wr = I.Wm + 3 * (size_t)(r + 1);
 #pragma unroll
@@ -921,6 +963,41 @@ __device__ __noinline__ void lo_chunk_recover(WarpSmem& w, int kc, int z, int m)
         atomic_max_nonneg(&h[1], b);
         if (kc == 0) I.lo_run[(size_t)z * I.lo_iter + m] = 1;
     }
+    if (next == nullptr) return;
+    // neighbours of every row (all lanes shuffle; the mask is the full warp)
+    double wl[3], wr[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        wl[q] = __shfl_up_sync(0xffffffffu, x[q], 1);
+        wr[q] = __shfl_down_sync(0xffffffffu, x[q], 1);
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) wl[q] = kc > 0 ? xl[q] : __ldcg(&I.Wm[q]);
+    }
+    if (lane == len - 1) {
+        if (kc + 1 < I.lo_k) {
+            const int s2 = e + 1;
+            const int e2 = (s2 + I.lo_len < I.n_inner ? s2 + I.lo_len : I.n_inner) - 1;
+            double xr2[3];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) xr2[q] = __ldcg(&I.xi[3 * (size_t)(kc + 1) + q]);
+            if (s2 == e2) {
+#pragma unroll
+                for (int q = 0; q < 3; ++q) wr[q] = xr2[q];
+            } else {
+                double o13[13];
+                rep_load(cur + 13 * (size_t)s2, o13);
+                rep_apply(o13, xr, xr2, wr);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) wr[q] = __ldcg(&I.Wm[3 * (size_t)(I.nx - 1) + q]);
+        }
+    }
+    LoRow L{};
+    if (lane < len) lo_row_w(I, r, wl, x, wr, L);
+    lo_chunk_solve(I, kc, L, next);
 }
 
 // ---- C: distribution solve over one tile (theta = 1/2) ------------------------
@@ -1329,14 +1406,17 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
             for (int b = threadIdx.x; b < n_inst && !lmine; b += kThreads)
                 lmine = lo_active(P.inst[b], z, m);
             if (!__syncthreads_or(lmine)) break;
-            if (m == 0) trace_h(P, z, 8, true);
-            // L1
-            for (long long u = gwarp; u < total_lo; u += nwarps) {
-                const int b = find_inst(P.lo_off, n_inst, u);
-                stage_warp(w, &P.inst[b], b);
-                if (!lo_active(w.I, z, m)) continue;
-                const int kc = (int)(u - w.I.lo_off);
-                if (m == 0) {
+            // representation sets: iteration m's in lorow set (m & 1)
+            const size_t set_cur = (size_t)(m & 1), set_next = (size_t)((m + 1) & 1);
+            // L1 (first LO iteration only; later ones are prepared by the
+            // fused recovery below)
+            if (m == 0) {
+                trace_h(P, z, 8, true);
+                for (long long u = gwarp; u < total_lo; u += nwarps) {
+                    const int b = find_inst(P.lo_off, n_inst, u);
+                    stage_warp(w, &P.inst[b], b);
+                    if (!lo_active(w.I, z, m)) continue;
+                    const int kc = (int)(u - w.I.lo_off);
                     const int s0 = kc * w.I.lo_len;
                     const int e0 = (s0 + w.I.lo_len < w.I.n_inner ? s0 + w.I.lo_len : w.I.n_inner);
                     double mx = 0.0;
@@ -1344,11 +1424,11 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
                     mx = warp_max(mx);
                     if (lane == 0) atomic_max_nonneg(&w.I.ho_red[4 * z + 3], mx);
                     __syncwarp();
+                    lo_chunk_eliminate(w, kc, w.I.lorow);
                 }
-                lo_chunk_eliminate(w, kc);
+                trace_h(P, z, 9, false);
+                if (!holo_sync(P, G)) return;
             }
-            if (m == 0) trace_h(P, z, 9, false);
-            if (!holo_sync(P, G)) return;
             if (m == 0) trace_h(P, z, 10, true);
             // L2: one CTA per instance
             if (lane == 0) w.cur_b = -1;  // shared memory is reused below
@@ -1356,7 +1436,7 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
             for (int b = blockIdx.x; b < n_inst; b += G) {
                 const HoloInst& I = P.inst[b];
                 if (!lo_active(I, z, m)) continue;
-                lo_reduced_solve(I, smem_raw);
+                lo_reduced_solve(I, I.lorow + set_cur * 13 * (size_t)I.n_inner, smem_raw);
             }
             __syncthreads();
             if (lane == 0) w.cur_b = -1;
@@ -1364,12 +1444,16 @@ __global__ void __launch_bounds__(kThreads, 3) holo_step_kernel(HoloDev* __restr
             if (m == 0) trace_h(P, z, 11, false);
             if (!holo_sync(P, G)) return;
             if (m == 0) trace_h(P, z, 12, true);
-            // L3
+            // L3 of iteration m fused with L1 of iteration m+1
             for (long long u = gwarp; u < total_lo; u += nwarps) {
                 const int b = find_inst(P.lo_off, n_inst, u);
                 stage_warp(w, &P.inst[b], b);
                 if (!lo_active(w.I, z, m)) continue;
-                lo_chunk_recover(w, (int)(u - w.I.lo_off), z, m);
+                const HoloInst& I = w.I;
+                const bool more = m + 1 < I.lo_iter && (I.fixed_lo <= 0 || m + 1 < I.fixed_lo);
+                lo_chunk_step(w, (int)(u - I.lo_off), z, m,
+                              I.lorow + set_cur * 13 * (size_t)I.n_inner,
+                              more ? I.lorow + set_next * 13 * (size_t)I.n_inner : nullptr);
             }
             if (m == 0) trace_h(P, z, 13, false);
             if (!holo_sync(P, G)) return;
@@ -1560,7 +1644,7 @@ size_t carve_holo(void* base, int nx, int nv, int kp, const keq_holo_params& p, 
     double* Ib = c.take<double>(8);
     double* Y = c.take<double>(3 * (size_t)nx);
     double* T1 = c.take<double>(3 * (size_t)nx);
-    double* lorow = c.take<double>(13 * (size_t)d.n_inner);
+    double* lorow = c.take<double>(2 * 13 * (size_t)d.n_inner);
     double* loedge = c.take<double>(18 * (size_t)d.lo_k);
     double* xi = c.take<double>(3 * (size_t)d.lo_k);
     double* agg = c.take<double>(ntiles * 64);
