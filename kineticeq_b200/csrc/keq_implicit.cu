@@ -586,6 +586,21 @@ __device__ __forceinline__ void write_tile(WarpSmem& w, int vt, int c, double* _
     }
 }
 
+// Element j of a small register array (a select chain, so the array stays
+// in registers), and its assignment.
+__device__ __forceinline__ double pick8(const double* a, int j) {
+    double v = 0.0;
+#pragma unroll
+    for (int k = 0; k < kMaxAACols; ++k)
+        if (k == j) v = a[k];
+    return v;
+}
+__device__ __forceinline__ void set8(double* a, int j, double v) {
+#pragma unroll
+    for (int k = 0; k < kMaxAACols; ++k)
+        if (k == j) a[k] = v;
+}
+
 // ---- Anderson: small symmetric solve (Cholesky, min-norm fall-back) -------
 // torch.linalg.cholesky / cholesky_solve with the lstsq fall-back of
 // bgk1d_aa_cpu.py:93-97; the fall-back here is a Jacobi eigen pseudo-inverse.
@@ -667,49 +682,102 @@ __device__ __noinline__ void aa_small_solve(int m, double* A, double* x) {
 }
 
 // Last reduction block of Anderson call m: Gram matrix from the per-block
-// partials (lane L sums blocks L, L+32, ...; fixed butterfly across lanes),
+// partials (lane q sums pair q over the row blocks in block order, 16 loads in
+// flight; the sums go through the warp's scratch `gs` in shared memory),
 // regularised Cholesky solve, normalisation by the sum, clip
 // (bgk1d_aa_cpu.py:146-168).
 __device__ __noinline__ void aa_finalize(const double* gpart, int nrb, int mh, double reg,
-                                         double alpha_max, double* alpha_out) {
+                                         double alpha_max, double* alpha_out, double* gs) {
     const int lane = threadIdx.x & 31;
-    double A[kMaxAACols * kMaxAACols];
-    // every pair's sum over the row blocks: lane L takes blocks L, L+32, ...
-    // with all pairs of a block loaded at once, then a fixed butterfly
     const int npairs = mh * (mh + 1) / 2;
-    double acc[kMaxPairs];
+    for (int q0 = 0; q0 < npairs; q0 += 32) {
+        const int q = q0 + lane;
+        double acc = 0.0;
+        for (int r0 = 0; r0 < nrb; r0 += 16) {
+            double t[16];
 #pragma unroll
-    for (int q = 0; q < kMaxPairs; ++q) acc[q] = 0.0;
-    for (int r2 = lane; r2 < nrb; r2 += 32) {
-        const double* gp = gpart + (size_t)r2 * kMaxPairs;
-        double t[kMaxPairs];
+            for (int u = 0; u < 16; ++u)
+                t[u] = (q < npairs && r0 + u < nrb) ? ld_cg(&gpart[(size_t)(r0 + u) * kMaxPairs + q])
+                                                    : 0.0;
 #pragma unroll
-        for (int q = 0; q < kMaxPairs; ++q) t[q] = q < npairs ? ld_cg(&gp[q]) : 0.0;
-#pragma unroll
-        for (int q = 0; q < kMaxPairs; ++q) acc[q] += t[q];
-    }
-#pragma unroll
-    for (int q = 0; q < kMaxPairs; ++q)
-        if (q < npairs) acc[q] = warp_sum(acc[q]);
-    int pj = 0;
-    for (int p = 0; p < mh; ++p)
-        for (int q = p; q < mh; ++q, ++pj) {
-            double sv = 0.0;
-#pragma unroll
-            for (int u = 0; u < kMaxPairs; ++u)
-                if (u == pj) sv = acc[u];
-            A[p * mh + q] = sv;
-            A[q * mh + p] = sv;
+            for (int u = 0; u < 16; ++u) acc += t[u];
         }
-    if (lane == 0) {
-        for (int p = 0; p < mh; ++p) A[p * mh + p] += reg;
+        if (q < npairs) gs[q] = acc;
+    }
+    __syncwarp();
+    // lane i (< mh) holds row i of the regularised Gram matrix
+    double Ai[kMaxAACols];
+#pragma unroll
+    for (int j = 0; j < kMaxAACols; ++j) {
+        const int p = lane < j ? lane : j, q = lane < j ? j : lane;
+        const int pi = p * mh - (p * (p - 1)) / 2 + (q - p);  // upper-triangle pair index
+        Ai[j] = (lane < mh && j < mh) ? gs[pi] : 0.0;
+        if (j == lane && lane < mh) Ai[j] += reg;
+    }
+    // Cholesky A = L L^T, lane i computing row i of L; every sum runs in the
+    // order of the serial routine (aa_small_solve), so the result is the same
+    double Li[kMaxAACols];
+#pragma unroll
+    for (int k = 0; k < kMaxAACols; ++k) Li[k] = 0.0;
+    bool ok = true;
+    for (int j = 0; j < mh; ++j) {
+        double Lj[kMaxAACols];
+#pragma unroll
+        for (int k = 0; k < kMaxAACols; ++k) Lj[k] = __shfl_sync(0xffffffffu, Li[k], j);
+        double sd = __shfl_sync(0xffffffffu, pick8(Ai, j), j);
+#pragma unroll
+        for (int k = 0; k < kMaxAACols; ++k)
+            if (k < j) sd -= Lj[k] * Lj[k];
+        if (!(sd > 0.0)) {
+            ok = false;
+            break;
+        }
+        const double ljj = sqrt(sd);
+        double t = pick8(Ai, j);
+#pragma unroll
+        for (int k = 0; k < kMaxAACols; ++k)
+            if (k < j) t -= Li[k] * Lj[k];
+        const double lij = lane > j ? t / ljj : ljj;
+        if (lane >= j && lane < mh) set8(Li, j, lij);
+    }
+    double xv[kMaxAACols];
+#pragma unroll
+    for (int k = 0; k < kMaxAACols; ++k) xv[k] = 0.0;
+    if (ok) {
+        // L y = 1, then L^T x = y
+        double yv[kMaxAACols];
+#pragma unroll
+        for (int k = 0; k < kMaxAACols; ++k) yv[k] = 0.0;
+        for (int i = 0; i < mh; ++i) {
+            double t = 1.0;
+#pragma unroll
+            for (int k = 0; k < kMaxAACols; ++k)
+                if (k < i) t -= Li[k] * yv[k];
+            const double yi = __shfl_sync(0xffffffffu, t / pick8(Li, i), i);
+            set8(yv, i, yi);
+        }
+        for (int i = mh - 1; i >= 0; --i) {
+            const double li = pick8(Li, i);
+            double t = pick8(yv, i);
+            for (int k = i + 1; k < mh; ++k) t -= __shfl_sync(0xffffffffu, li, k) * pick8(xv, k);
+            set8(xv, i, t / __shfl_sync(0xffffffffu, li, i));
+        }
+    } else {
+        // not positive definite: the serial routine's min-norm fall-back on
+        // the full matrix, gathered from the lanes' rows
+        double A[kMaxAACols * kMaxAACols];
+        for (int p = 0; p < mh; ++p)
+            for (int q = 0; q < mh; ++q) A[p * mh + q] = __shfl_sync(0xffffffffu, pick8(Ai, q), p);
         double al[kMaxAACols];
-        aa_small_solve(mh, A, al);
+        if (lane == 0) aa_small_solve(mh, A, al);
+        for (int p = 0; p < mh; ++p) set8(xv, p, __shfl_sync(0xffffffffu, al[p], 0));
+    }
+    if (lane == 0) {
         double asum = 0.0;
-        for (int p = 0; p < mh; ++p) asum += al[p];
+        for (int p = 0; p < mh; ++p) asum += pick8(xv, p);
         if (fabs(asum) < 1.0e-30) asum = 1.0e-30;
         for (int p = 0; p < mh; ++p) {
-            double a = al[p] / asum;
+            double a = pick8(xv, p) / asum;
             if (alpha_max > 0.0) {
                 if (a < -alpha_max) a = -alpha_max;
                 if (a > alpha_max) a = alpha_max;
@@ -824,7 +892,7 @@ __device__ __noinline__ void reduce_block(WarpSmem& w, int ru, int m) {
                 fence_acq_rel();
                 __syncwarp();
                 aa_finalize(I.gpart, I.nrb, mh, I.aa_reg, I.aa_alpha_max,
-                            I.alpha + (size_t)m * kMaxAACols);
+                            I.alpha + (size_t)m * kMaxAACols, &w.coef[0][0]);
             }
         }
     }
