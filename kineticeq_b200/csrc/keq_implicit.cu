@@ -860,29 +860,36 @@ __device__ __noinline__ void reduce_block(WarpSmem& w, int ru, int m) {
         }
         if (aa_applies(I, m)) {
             plain = false;
-            double rv[kMaxAACols][3];
-#pragma unroll
-            for (int jj = 0; jj < kMaxAACols; ++jj) {
+            // the block's residual history r_j (3 components per row) in the
+            // warp's tile buffer (free here): row = lane, column 3 j + c
+            for (int jj = 0; jj < mh; ++jj) {
                 const int col = ((head_out - mh + jj) % I.aa_cols + I.aa_cols) % I.aa_cols;
 #pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    rv[jj][q] = 0.0;
-                    if (ok && jj < mh)
-                        rv[jj][q] = (col == head_in) ? (wn[q] - wo[q])
-                                                     : ld_cg(&I.aaR[(size_t)col * d + q * n_inner + k]);
-                }
+                for (int q = 0; q < 3; ++q)
+                    w.a[lane][3 * jj + q] =
+                        !ok ? 0.0
+                            : (col == head_in ? (wn[q] - wo[q])
+                                              : ld_cg(&I.aaR[(size_t)col * d + q * n_inner + k]));
             }
-#pragma unroll
-            for (int p = 0; p < kMaxAACols; ++p)
-#pragma unroll
-                for (int q = p; q < kMaxAACols; ++q) {
-                    if (p < mh && q < mh) {
-                        const double v = warp_sum(rv[p][0] * rv[q][0] + rv[p][1] * rv[q][1] +
-                                                  rv[p][2] * rv[q][2]);
-                        const int pi = p * mh - (p * (p - 1)) / 2 + (q - p);
-                        if (lane == 0) I.gpart[(size_t)ru * kMaxPairs + pi] = v;
-                    }
+            __syncwarp();
+            // Gram partials of the block: lane t sums pair t = (p, q) over the
+            // block's rows in row order
+            const int npairs = mh * (mh + 1) / 2;
+            for (int t = lane; t < npairs; t += 32) {
+                int p = 0, rem = t;
+                while (rem >= mh - p) {
+                    rem -= mh - p;
+                    ++p;
                 }
+                const int q = p + rem;
+                double v = 0.0;
+#pragma unroll 8
+                for (int r = 0; r < kRB; ++r)
+                    v += w.a[r][3 * p] * w.a[r][3 * q] + w.a[r][3 * p + 1] * w.a[r][3 * q + 1] +
+                         w.a[r][3 * p + 2] * w.a[r][3 * q + 2];
+                I.gpart[(size_t)ru * kMaxPairs + t] = v;
+            }
+            __syncwarp();
             fence_acq_rel();
             __syncwarp();
             unsigned prev = 0;
