@@ -25,6 +25,15 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+// Polling load without ordering; a wait that ends on it is followed by
+// fence_gpu() (relaxed load + fence = acquire), so each poll costs no L1
+// invalidation.
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void fence_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
@@ -170,10 +179,11 @@ __device__ __forceinline__ double warp_max(double v) {
 // the k-th barrier is passed once the counter reaches k * nblocks, and an
 // arriving CTA learns k from the value its own arrival returns (arrivals of
 // barrier k lie in [(k-1) nblocks, k nblocks) because no CTA can arrive at
-// barrier k+1 before barrier k is passed).  The arrival is a release and the
-// wait an acquire at gpu scope, so stores made by any thread of any CTA before
+// barrier k+1 before barrier k is passed).  The arrival is a release; the
+// wait polls relaxed and ends with an acq_rel fence (the last arriver, which
+// does not wait, fences too), so stores made by any thread of any CTA before
 // the barrier are visible to every thread after it (the CTA's bar.sync
-// carries the ordering to and from thread 0); the acquire also invalidates
+// carries the ordering to and from thread 0); the fence also invalidates
 // the SM's L1 for the ordinary loads that follow.  No word is reset between
 // barriers, which saves the release round trip of a generation counter.
 // Every wait is bounded: on timeout the CTA records KEQ_ERR_TIMEOUT in *err
@@ -200,7 +210,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned nblocks, int
         if (old + 1u != target) {
             unsigned long long it = 0;
             unsigned ns = 0;
-            while ((int)(ld_acquire(&gb->count) - target) < 0) {
+            while ((int)(ld_relaxed(&gb->count) - target) < 0) {
                 if (++it > limit) {
                     atomicOr(err, 1 << KEQ_ERR_TIMEOUT);
                     ok = 0;
@@ -210,6 +220,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned nblocks, int
                 ns = ns ? (ns < 128 ? 2 * ns : ns) : 16;
             }
         }
+        if (ok) fence_gpu();
         s_ok = ok;
     }
     __syncthreads();
@@ -238,7 +249,7 @@ __device__ __forceinline__ bool wait_flag_geq(const unsigned* flag, unsigned wan
                                               unsigned long long limit = kSpinLimit) {
     unsigned long long it = 0;
     unsigned ns = 16;
-    while (ld_acquire(flag) < want) {
+    while (ld_relaxed(flag) < want) {
         if (++it > limit) {
             atomicOr(err, 1 << KEQ_ERR_TIMEOUT);
             return false;
@@ -246,6 +257,7 @@ __device__ __forceinline__ bool wait_flag_geq(const unsigned* flag, unsigned wan
         __nanosleep(ns);
         if (ns < 128) ns <<= 1;
     }
+    fence_gpu();
     return true;
 }
 

@@ -89,7 +89,7 @@ struct ImpInst {
     int* nonfin;     // picard_iter   : non-finite flag of iterate m+1
     double* aaG;     // aa_cols * 3*n_inner
     double* aaR;     // aa_cols * 3*n_inner
-    double* gpart;   // nrb * kMaxPairs
+    double* gpart;   // kMaxPairs * nrb : Gram partials of the row blocks, pair-major
     double* alpha;   // picard_iter * kMaxAACols
     unsigned* rbdone;// picard_iter
     float* fn32;     // nx*nv (mixed form): f^n in FP32, written by P1
@@ -681,110 +681,136 @@ __device__ __noinline__ void aa_small_solve(int m, double* A, double* x) {
     }
 }
 
+// Index of pair (p, q), p <= q, in the row-major upper triangle of an m x m
+// symmetric matrix.
+__host__ __device__ constexpr int aa_pair(int p, int q, int m) {
+    return p * m - (p * (p - 1)) / 2 + (q - p);
+}
+__device__ __forceinline__ double aa_clip(double a, double alpha_max) {
+    if (alpha_max > 0.0) {
+        if (a < -alpha_max) a = -alpha_max;
+        if (a > alpha_max) a = alpha_max;
+    }
+    return a;
+}
+
+// Anderson coefficients for a history of compile-time length M in one thread,
+// the factor in registers: (G + reg I) x = 1 by Cholesky with the sums in the
+// order of aa_small_solve, then alpha = x / sum(x), clipped
+// (bgk1d_aa_cpu.py:146-168).  Each pivot is kept as its reciprocal square
+// root and the divisions by it are multiplications, so the dependent chain of
+// a column is one rsqrt.  False (nothing written) when a pivot is not
+// positive, for the min-norm fall-back.
+template <int M>
+__device__ __forceinline__ bool aa_alpha_fixed(const double* gs, double reg, double alpha_max,
+                                               double* alpha_out) {
+    double L[M][M], rd[M];  // strict lower factor; rd[j] = 1 / L[j][j]
+#pragma unroll
+    for (int i = 0; i < M; ++i)
+#pragma unroll
+        for (int j = 0; j <= i; ++j) L[i][j] = gs[aa_pair(j, i, M)] + (i == j ? reg : 0.0);
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+        double s = L[j][j];
+#pragma unroll
+        for (int k = 0; k < j; ++k) s -= L[j][k] * L[j][k];
+        if (!(s > 0.0)) return false;
+        rd[j] = rsqrt(s);
+#pragma unroll
+        for (int i = j + 1; i < M; ++i) {
+            double t = L[i][j];
+#pragma unroll
+            for (int k = 0; k < j; ++k) t -= L[i][k] * L[j][k];
+            L[i][j] = t * rd[j];
+        }
+    }
+    double y[M], x[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        double t = 1.0;
+#pragma unroll
+        for (int k = 0; k < i; ++k) t -= L[i][k] * y[k];
+        y[i] = t * rd[i];
+    }
+#pragma unroll
+    for (int i = M - 1; i >= 0; --i) {
+        double t = y[i];
+#pragma unroll
+        for (int k = i + 1; k < M; ++k) t -= L[k][i] * x[k];
+        x[i] = t * rd[i];
+    }
+    double asum = 0.0;
+#pragma unroll
+    for (int p = 0; p < M; ++p) asum += x[p];
+    if (fabs(asum) < 1.0e-30) asum = 1.0e-30;
+    const double rs = 1.0 / asum;
+#pragma unroll
+    for (int p = 0; p < M; ++p) alpha_out[p] = aa_clip(x[p] * rs, alpha_max);
+    return true;
+}
+
 // Last reduction block of Anderson call m: Gram matrix from the per-block
-// partials (lane q sums pair q over the row blocks in block order, 16 loads in
-// flight; the sums go through the warp's scratch `gs` in shared memory),
+// partials, stored pair-major (lane l sums blocks l, l+32, ... of eight pairs
+// at a time, 32 loads in flight, then a butterfly over the lanes; the sums go
+// through the warp's scratch `gs` in shared memory),
 // regularised Cholesky solve, normalisation by the sum, clip
 // (bgk1d_aa_cpu.py:146-168).
 __device__ __noinline__ void aa_finalize(const double* gpart, int nrb, int mh, double reg,
                                          double alpha_max, double* alpha_out, double* gs) {
     const int lane = threadIdx.x & 31;
     const int npairs = mh * (mh + 1) / 2;
-    for (int q0 = 0; q0 < npairs; q0 += 32) {
-        const int q = q0 + lane;
-        double acc = 0.0;
-        for (int r0 = 0; r0 < nrb; r0 += 16) {
-            double t[16];
+    for (int q0 = 0; q0 < npairs; q0 += 8) {
+        double acc[8];
 #pragma unroll
-            for (int u = 0; u < 16; ++u)
-                t[u] = (q < npairs && r0 + u < nrb) ? ld_cg(&gpart[(size_t)(r0 + u) * kMaxPairs + q])
-                                                    : 0.0;
+        for (int u = 0; u < 8; ++u) acc[u] = 0.0;
+        for (int r0 = 0; r0 < nrb; r0 += 128) {
+            double t[8][4];
 #pragma unroll
-            for (int u = 0; u < 16; ++u) acc += t[u];
+            for (int u = 0; u < 8; ++u)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const int r = r0 + 32 * c + lane;
+                    t[u][c] = (q0 + u < npairs && r < nrb) ? ld_cg(&gpart[(size_t)(q0 + u) * nrb + r])
+                                                           : 0.0;
+                }
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[u] += t[u][c];
         }
-        if (q < npairs) gs[q] = acc;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) acc[u] = warp_sum(acc[u]);
+        if (lane == 0)
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (q0 + u < npairs) gs[q0 + u] = acc[u];
     }
     __syncwarp();
-    // lane i (< mh) holds row i of the regularised Gram matrix
-    double Ai[kMaxAACols];
-#pragma unroll
-    for (int j = 0; j < kMaxAACols; ++j) {
-        const int p = lane < j ? lane : j, q = lane < j ? j : lane;
-        const int pi = p * mh - (p * (p - 1)) / 2 + (q - p);  // upper-triangle pair index
-        Ai[j] = (lane < mh && j < mh) ? gs[pi] : 0.0;
-        if (j == lane && lane < mh) Ai[j] += reg;
+    if (lane != 0) return;
+    bool ok = false;
+    switch (mh) {
+        case 1: ok = aa_alpha_fixed<1>(gs, reg, alpha_max, alpha_out); break;
+        case 2: ok = aa_alpha_fixed<2>(gs, reg, alpha_max, alpha_out); break;
+        case 3: ok = aa_alpha_fixed<3>(gs, reg, alpha_max, alpha_out); break;
+        case 4: ok = aa_alpha_fixed<4>(gs, reg, alpha_max, alpha_out); break;
+        case 5: ok = aa_alpha_fixed<5>(gs, reg, alpha_max, alpha_out); break;
+        case 6: ok = aa_alpha_fixed<6>(gs, reg, alpha_max, alpha_out); break;
+        case 7: ok = aa_alpha_fixed<7>(gs, reg, alpha_max, alpha_out); break;
+        default: ok = aa_alpha_fixed<8>(gs, reg, alpha_max, alpha_out); break;
     }
-    // Cholesky A = L L^T, lane i computing row i of L; every sum runs in the
-    // order of the serial routine (aa_small_solve), so the result is the same
-    double Li[kMaxAACols];
-#pragma unroll
-    for (int k = 0; k < kMaxAACols; ++k) Li[k] = 0.0;
-    bool ok = true;
-    for (int j = 0; j < mh; ++j) {
-        double Lj[kMaxAACols];
-#pragma unroll
-        for (int k = 0; k < kMaxAACols; ++k) Lj[k] = __shfl_sync(0xffffffffu, Li[k], j);
-        double sd = __shfl_sync(0xffffffffu, pick8(Ai, j), j);
-#pragma unroll
-        for (int k = 0; k < kMaxAACols; ++k)
-            if (k < j) sd -= Lj[k] * Lj[k];
-        if (!(sd > 0.0)) {
-            ok = false;
-            break;
+    if (ok) return;
+    // not positive definite: the min-norm fall-back on the full matrix
+    double A[kMaxAACols * kMaxAACols], xv[kMaxAACols];
+    for (int p = 0; p < mh; ++p)
+        for (int q = 0; q < mh; ++q) {
+            const int a = p < q ? p : q, b = p < q ? q : p;
+            A[p * mh + q] = gs[aa_pair(a, b, mh)] + (p == q ? reg : 0.0);
         }
-        const double ljj = sqrt(sd);
-        double t = pick8(Ai, j);
-#pragma unroll
-        for (int k = 0; k < kMaxAACols; ++k)
-            if (k < j) t -= Li[k] * Lj[k];
-        const double lij = lane > j ? t / ljj : ljj;
-        if (lane >= j && lane < mh) set8(Li, j, lij);
-    }
-    double xv[kMaxAACols];
-#pragma unroll
-    for (int k = 0; k < kMaxAACols; ++k) xv[k] = 0.0;
-    if (ok) {
-        // L y = 1, then L^T x = y
-        double yv[kMaxAACols];
-#pragma unroll
-        for (int k = 0; k < kMaxAACols; ++k) yv[k] = 0.0;
-        for (int i = 0; i < mh; ++i) {
-            double t = 1.0;
-#pragma unroll
-            for (int k = 0; k < kMaxAACols; ++k)
-                if (k < i) t -= Li[k] * yv[k];
-            const double yi = __shfl_sync(0xffffffffu, t / pick8(Li, i), i);
-            set8(yv, i, yi);
-        }
-        for (int i = mh - 1; i >= 0; --i) {
-            const double li = pick8(Li, i);
-            double t = pick8(yv, i);
-            for (int k = i + 1; k < mh; ++k) t -= __shfl_sync(0xffffffffu, li, k) * pick8(xv, k);
-            set8(xv, i, t / __shfl_sync(0xffffffffu, li, i));
-        }
-    } else {
-        // not positive definite: the serial routine's min-norm fall-back on
-        // the full matrix, gathered from the lanes' rows
-        double A[kMaxAACols * kMaxAACols];
-        for (int p = 0; p < mh; ++p)
-            for (int q = 0; q < mh; ++q) A[p * mh + q] = __shfl_sync(0xffffffffu, pick8(Ai, q), p);
-        double al[kMaxAACols];
-        if (lane == 0) aa_small_solve(mh, A, al);
-        for (int p = 0; p < mh; ++p) set8(xv, p, __shfl_sync(0xffffffffu, al[p], 0));
-    }
-    if (lane == 0) {
-        double asum = 0.0;
-        for (int p = 0; p < mh; ++p) asum += pick8(xv, p);
-        if (fabs(asum) < 1.0e-30) asum = 1.0e-30;
-        for (int p = 0; p < mh; ++p) {
-            double a = pick8(xv, p) / asum;
-            if (alpha_max > 0.0) {
-                if (a < -alpha_max) a = -alpha_max;
-                if (a > alpha_max) a = alpha_max;
-            }
-            alpha_out[p] = a;
-        }
-    }
+    aa_small_solve(mh, A, xv);
+    double asum = 0.0;
+    for (int p = 0; p < mh; ++p) asum += xv[p];
+    if (fabs(asum) < 1.0e-30) asum = 1.0e-30;
+    for (int p = 0; p < mh; ++p) alpha_out[p] = aa_clip(xv[p] / asum, alpha_max);
 }
 
 // ---- row reduction / W update of one row block (lane = row) -------------
@@ -795,14 +821,37 @@ __device__ __noinline__ void reduce_block(WarpSmem& w, int ru, int m) {
     const bool ok = k < I.n_inner;
     const int i = k + 1;
     const int nx = I.nx, n_inner = I.n_inner, d = 3 * n_inner;
+    // Anderson call m: history column head_in = m % cols, length min(m+1, cols)
+    const bool aa_now = aa_applies(I, m);
+    const int cols = I.aa_cols > 0 ? I.aa_cols : 1;
+    const int head_in = m % cols;
+    const int mh = (m + 1) < cols ? (m + 1) : cols;
+    const int head_out = (m + 1) % cols;
+    if (aa_now) {
+        // the block's older residual columns r_j (3 components per row) into
+        // the warp's tile buffer (free here; row = lane, column 3 j + c),
+        // copied while the moment partials are read; the newest column
+        // (jj = mh - 1, slot head_in) is formed below
+        int col = ((head_out - mh) % cols + cols) % cols;
+        for (int jj = 0; jj < mh - 1; ++jj) {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                if (ok)
+                    cp_async8(&w.a[lane][3 * jj + q], &I.aaR[(size_t)col * d + q * n_inner + k]);
+                else
+                    w.a[lane][3 * jj + q] = 0.0;
+            }
+            col = col + 1 == cols ? 0 : col + 1;
+        }
+    }
     double wn[3] = {0.0, 0.0, 0.0}, wo[3] = {0.0, 0.0, 0.0};
     if (ok) {
-        double s[4];
-        sum_partials4(I.part, 0, I.nvt, n_inner, k, s);
-        moments_from_sums(s[0], s[1], s[2], I.dv, &wn[0], &wn[1], &wn[2]);
         wo[0] = ld_cg(&I.W[i]);
         wo[1] = ld_cg(&I.W[nx + i]);
         wo[2] = ld_cg(&I.W[2 * nx + i]);
+        double s[4];
+        sum_partials4(I.part, 0, I.nvt, n_inner, k, s);
+        moments_from_sums(s[0], s[1], s[2], I.dv, &wn[0], &wn[1], &wn[2]);
         I.Wn[i] = wn[0];
         I.Wn[nx + i] = wn[1];
         I.Wn[2 * nx + i] = wn[2];
@@ -847,10 +896,6 @@ __device__ __noinline__ void reduce_block(WarpSmem& w, int ru, int m) {
 
     bool plain = true;
     if (I.aa_on) {
-        // Anderson call m: history column head_in = m % cols, length min(m+1, cols)
-        const int head_in = m % I.aa_cols;
-        const int mh = (m + 1) < I.aa_cols ? (m + 1) : I.aa_cols;
-        const int head_out = (m + 1) % I.aa_cols;
         if (ok) {
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
@@ -858,19 +903,11 @@ __device__ __noinline__ void reduce_block(WarpSmem& w, int ru, int m) {
                 I.aaR[(size_t)head_in * d + q * n_inner + k] = wn[q] - wo[q];
             }
         }
-        if (aa_applies(I, m)) {
+        if (aa_now) {
             plain = false;
-            // the block's residual history r_j (3 components per row) in the
-            // warp's tile buffer (free here): row = lane, column 3 j + c
-            for (int jj = 0; jj < mh; ++jj) {
-                const int col = ((head_out - mh + jj) % I.aa_cols + I.aa_cols) % I.aa_cols;
 #pragma unroll
-                for (int q = 0; q < 3; ++q)
-                    w.a[lane][3 * jj + q] =
-                        !ok ? 0.0
-                            : (col == head_in ? (wn[q] - wo[q])
-                                              : ld_cg(&I.aaR[(size_t)col * d + q * n_inner + k]));
-            }
+            for (int q = 0; q < 3; ++q) w.a[lane][3 * (mh - 1) + q] = ok ? wn[q] - wo[q] : 0.0;
+            cp_async_wait_all();
             __syncwarp();
             // Gram partials of the block: lane t sums pair t = (p, q) over the
             // block's rows in row order
@@ -887,7 +924,7 @@ __device__ __noinline__ void reduce_block(WarpSmem& w, int ru, int m) {
                 for (int r = 0; r < kRB; ++r)
                     v += w.a[r][3 * p] * w.a[r][3 * q] + w.a[r][3 * p + 1] * w.a[r][3 * q + 1] +
                          w.a[r][3 * p + 2] * w.a[r][3 * q + 2];
-                I.gpart[(size_t)ru * kMaxPairs + t] = v;
+                I.gpart[(size_t)t * I.nrb + ru] = v;
             }
             __syncwarp();
             fence_acq_rel();
@@ -1125,10 +1162,12 @@ implicit_step_kernel(PlanDev* __restrict__ Pp, int swap_io) {
                 rowblock_arrive(w.I.rbcnt + (size_t)m * w.I.nrb, w.I.nx, w.I.n_inner, w.I.nvt, g,
                                 w.done_rb);
             __syncwarp();
-            write_tile(w, vt, c, fo, is32);
             const int d0 = w.done_rb[0], d1 = w.done_rb[1];
+            // acquire side of a completed block, before the tile's write-back
+            // so that the fence does not wait for those stores
+            if (d0 >= 0 || d1 >= 0) fence_acq_rel();
+            write_tile(w, vt, c, fo, is32);
             if (d0 >= 0 || d1 >= 0) {
-                fence_acq_rel();
                 __syncwarp();
                 if (d0 >= 0) reduce_block(w, d0, m);
                 if (d1 >= 0) reduce_block(w, d1, m);

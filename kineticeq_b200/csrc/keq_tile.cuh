@@ -33,9 +33,9 @@ constexpr int kWin = 32;    // predecessor chunks polled per look-back round
 constexpr int kPartQ = 4;   // doubles per (v-tile, row) partial: sum x, x v, x v^2, x v^3
 constexpr unsigned long long kFlagAgg = 1ull, kFlagInc = 2ull;
 
-__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long* p) {
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
     unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
 __device__ __forceinline__ void st_release64(unsigned long long* p, unsigned long long v) {
@@ -66,12 +66,15 @@ __device__ __forceinline__ TileGeo tile_geo(int nt_neg, int kp, int nv, int n_in
 __device__ __forceinline__ int scan_row(int nx, bool pos, int s) { return pos ? 1 + s : nx - 2 - s; }
 
 // Publish the tile's aggregate map (P, Y) (one value per lane/velocity).
+// The warp barrier orders every lane's stores before lane 0's flag store, and
+// a release is cumulative over what precedes it, so one release by lane 0
+// publishes the whole warp's values (the bar.sync + one-thread fence pattern
+// of a grid barrier, at warp level); no per-lane fence is needed.
 __device__ __forceinline__ void publish_agg(double* agg, unsigned long long* flag, size_t tid,
                                             double P, double Y, unsigned long long epoch) {
     const int lane = threadIdx.x & 31;
     __stcg(&agg[tid * 64 + lane], P);
     __stcg(&agg[tid * 64 + 32 + lane], Y);
-    fence_acq_rel();
     __syncwarp();
     if (lane == 0) st_release64(&flag[tid], (epoch << 2) | kFlagAgg);
 }
@@ -81,15 +84,15 @@ __device__ __forceinline__ void publish_inc(double* inc, unsigned long long* fla
                                             double X, unsigned long long epoch) {
     const int lane = threadIdx.x & 31;
     __stcg(&inc[tid * 32 + lane], X);
-    fence_acq_rel();
     __syncwarp();
     if (lane == 0) st_release64(&flag[tid], (epoch << 2) | kFlagInc);
 }
 
 // Carry into chunk c >= 1 of v-tile column vt (tile index t = chunk * nvt +
-// vt).  Lane q polls chunk c-1-q; the nearest chunk with an inclusive value
-// whose successors up to c-1 all have aggregates is the base.  Bounded: on
-// timeout returns false (X = 0).
+// vt).  Lane q polls chunk c-1-q (relaxed; the fence after the wait makes it
+// an acquire); the nearest chunk with an inclusive value whose successors up
+// to c-1 all have aggregates is the base.  Bounded: on timeout returns false
+// (X = 0).
 __device__ __forceinline__ bool lookback(const double* agg, const double* inc,
                                          const unsigned long long* flag, int nvt, int vt, int c,
                                          unsigned long long epoch, unsigned long long limit,
@@ -101,7 +104,7 @@ __device__ __forceinline__ bool lookback(const double* agg, const double* inc,
     int q = -1;
     for (;;) {
         unsigned long long f = 0ull;
-        if (lane < nval) f = ld_acquire64(&flag[(size_t)(c - 1 - lane) * nvt + vt]);
+        if (lane < nval) f = ld_relaxed64(&flag[(size_t)(c - 1 - lane) * nvt + vt]);
         const bool cur = (f >> 2) == epoch;
         const unsigned incm = __ballot_sync(0xffffffffu, cur && (f & 3ull) == kFlagInc);
         const unsigned aggm = __ballot_sync(0xffffffffu, cur && (f & 3ull) != 0ull);
@@ -117,8 +120,10 @@ __device__ __forceinline__ bool lookback(const double* agg, const double* inc,
         __nanosleep(ns);
         if (ns < 256) ns <<= 1;
     }
-    __syncwarp();
+    // the polling lanes' fence completes their acquire; the warp barrier then
+    // orders every lane's loads below after it
     fence_acq_rel();
+    __syncwarp();
     double x = __ldcg(&inc[((size_t)(c - 1 - q) * nvt + vt) * 32 + lane]);
     for (int k0 = q - 1; k0 >= 0; k0 -= 8) {
         double Pk[8], Yk[8];
@@ -166,14 +171,15 @@ __device__ __forceinline__ void row_sums4(const double (*buf)[33], const double*
 }
 
 // Sum of the per-v-tile partials of interior row k over the v-tiles
-// [vt0, vt1), in v-tile order (loads issued in batches of 8).
+// [vt0, vt1), in v-tile order (loads issued in batches of B).
+template <int B = 8>
 __device__ __forceinline__ void sum_partials4(const double* part, int vt0, int vt1, int n_inner,
                                               int k, double* s) {
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    for (int v0 = vt0; v0 < vt1; v0 += 8) {
-        double2 p01[8], p23[8];
+    for (int v0 = vt0; v0 < vt1; v0 += B) {
+        double2 p01[B], p23[B];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
+        for (int q = 0; q < B; ++q) {
             if (v0 + q < vt1) {
                 const double* p = part + ((size_t)(v0 + q) * n_inner + k) * kPartQ;
                 p01[q] = __ldcg(reinterpret_cast<const double2*>(p));
@@ -181,7 +187,7 @@ __device__ __forceinline__ void sum_partials4(const double* part, int vt0, int v
             }
         }
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
+        for (int q = 0; q < B; ++q) {
             if (v0 + q < vt1) {
                 a0 += p01[q].x;
                 a1 += p01[q].y;
