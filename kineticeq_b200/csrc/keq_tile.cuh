@@ -57,9 +57,17 @@ __device__ __forceinline__ TileGeo tile_geo(int nt_neg, int kp, int nv, int n_in
     g.pos = vt >= nt_neg;
     g.j = g.pos ? kp + 32 * (vt - nt_neg) + lane : kp - 32 * (vt + 1) + lane;
     g.lane_ok = g.pos ? (g.j < nv) : (g.j >= 0);
-    g.s0 = c * R;
-    const int rem = n_inner - g.s0;
-    g.nrows = rem < R ? rem : R;
+    // Chunks of R scan positions cut so that their interior rows start at
+    // multiples of R: a forward (v > 0) chunk c holds rows k in [cR, cR + R);
+    // a backward scan runs from k = n_inner - 1 down and its chunk 0 takes the
+    // remainder n_inner mod R, so that every later backward chunk starts at a
+    // multiple of R as well.  With R dividing the row-block size every tile
+    // then lies inside one row block.  Both directions have ceil(n_inner / R)
+    // chunks.
+    const int pad = g.pos ? 0 : (R - n_inner % R) % R;
+    g.s0 = c == 0 ? 0 : c * R - pad;
+    const int end = (c + 1) * R - pad;
+    g.nrows = (end < n_inner ? end : n_inner) - g.s0;
     return g;
 }
 
