@@ -320,12 +320,16 @@ __device__ __forceinline__ void stage_coeffs(WarpSmem& w, const TileGeo& g, int 
             const int k = i - 1, d = 3 * n_inner;
             const int mh = m < I.aa_cols ? m : I.aa_cols;
             const int head_out = m % I.aa_cols;
+            // every load is issued unconditionally (entries past the history
+            // length repeat its last column and are selected out of the sums),
+            // so that each batch is in flight together
             double al[kMaxAACols];
             int col[kMaxAACols];
 #pragma unroll
             for (int jj = 0; jj < kMaxAACols; ++jj) {
-                al[jj] = jj < mh ? ld_cg(&I.alpha[(size_t)(m - 1) * kMaxAACols + jj]) : 0.0;
-                col[jj] = ((head_out - mh + jj) % I.aa_cols + I.aa_cols) % I.aa_cols;
+                const int jc = jj < mh ? jj : mh - 1;
+                al[jj] = ld_cg(&I.alpha[(size_t)(m - 1) * kMaxAACols + jc]);
+                col[jj] = ((head_out - mh + jc) % I.aa_cols + I.aa_cols) % I.aa_cols;
             }
             double wv[3];
 #pragma unroll
@@ -333,12 +337,11 @@ __device__ __forceinline__ void stage_coeffs(WarpSmem& w, const TileGeo& g, int 
                 double gv[kMaxAACols];
 #pragma unroll
                 for (int jj = 0; jj < kMaxAACols; ++jj)
-                    gv[jj] = jj < mh ? ld_cg(&I.aaG[(size_t)col[jj] * d + q * n_inner + k]) : 0.0;
+                    gv[jj] = ld_cg(&I.aaG[(size_t)col[jj] * d + q * n_inner + k]);
+                const double wnew = ld_cg(&I.Wn[q * nx + i]);
                 double acc = 0.0;
 #pragma unroll
-                for (int jj = 0; jj < kMaxAACols; ++jj)
-                    if (jj < mh) acc += gv[jj] * al[jj];
-                const double wnew = ld_cg(&I.Wn[q * nx + i]);
+                for (int jj = 0; jj < kMaxAACols; ++jj) acc += jj < mh ? gv[jj] * al[jj] : 0.0;
                 wv[q] = acc * I.aa_beta + (1.0 - I.aa_beta) * wnew;
             }
             const double nm = clamp_min_t(wv[0], 1e-12);
@@ -769,9 +772,12 @@ __device__ __noinline__ void aa_finalize(const double* gpart, int nrb, int mh, d
             for (int u = 0; u < 8; ++u)
 #pragma unroll
                 for (int c = 0; c < 4; ++c) {
+                    // clamped indices: every load is issued, the extra ones add 0
                     const int r = r0 + 32 * c + lane;
-                    t[u][c] = (q0 + u < npairs && r < nrb) ? ld_cg(&gpart[(size_t)(q0 + u) * nrb + r])
-                                                           : 0.0;
+                    const bool in = q0 + u < npairs && r < nrb;
+                    const int qc = q0 + u < npairs ? q0 + u : npairs - 1;
+                    const double v = ld_cg(&gpart[(size_t)qc * nrb + (r < nrb ? r : nrb - 1)]);
+                    t[u][c] = in ? v : 0.0;
                 }
 #pragma unroll
             for (int u = 0; u < 8; ++u)

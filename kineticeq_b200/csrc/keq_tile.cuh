@@ -133,22 +133,23 @@ __device__ __forceinline__ bool lookback(const double* agg, const double* inc,
     fence_acq_rel();
     __syncwarp();
     double x = __ldcg(&inc[((size_t)(c - 1 - q) * nvt + vt) * 32 + lane]);
+    // eight predecessor maps per round, loaded unconditionally (an index past
+    // the first is clamped to it and its map replaced by the identity) so that
+    // all sixteen loads are in flight together
     for (int k0 = q - 1; k0 >= 0; k0 -= 8) {
         double Pk[8], Yk[8];
 #pragma unroll
         for (int t = 0; t < 8; ++t) {
-            Pk[t] = 1.0;
-            Yk[t] = 0.0;
-            const int k = k0 - t;
-            if (k >= 0) {
-                const size_t tid = (size_t)(c - 1 - k) * nvt + vt;
-                Pk[t] = __ldcg(&agg[tid * 64 + lane]);
-                Yk[t] = __ldcg(&agg[tid * 64 + 32 + lane]);
-            }
+            const int k = k0 - t >= 0 ? k0 - t : 0;
+            const size_t tid = (size_t)(c - 1 - k) * nvt + vt;
+            Pk[t] = __ldcg(&agg[tid * 64 + lane]);
+            Yk[t] = __ldcg(&agg[tid * 64 + 32 + lane]);
         }
 #pragma unroll
-        for (int t = 0; t < 8; ++t)
-            if (k0 - t >= 0) x = fma(Pk[t], x, Yk[t]);
+        for (int t = 0; t < 8; ++t) {
+            const bool use = k0 - t >= 0;
+            x = fma(use ? Pk[t] : 1.0, x, use ? Yk[t] : 0.0);
+        }
     }
     X = x;
     return true;
@@ -188,20 +189,18 @@ __device__ __forceinline__ void sum_partials4(const double* part, int vt0, int v
         double2 p01[B], p23[B];
 #pragma unroll
         for (int q = 0; q < B; ++q) {
-            if (v0 + q < vt1) {
-                const double* p = part + ((size_t)(v0 + q) * n_inner + k) * kPartQ;
-                p01[q] = __ldcg(reinterpret_cast<const double2*>(p));
-                p23[q] = __ldcg(reinterpret_cast<const double2*>(p + 2));
-            }
+            const int v = v0 + q < vt1 ? v0 + q : vt1 - 1;  // clamped: every load is issued
+            const double* p = part + ((size_t)v * n_inner + k) * kPartQ;
+            p01[q] = __ldcg(reinterpret_cast<const double2*>(p));
+            p23[q] = __ldcg(reinterpret_cast<const double2*>(p + 2));
         }
 #pragma unroll
         for (int q = 0; q < B; ++q) {
-            if (v0 + q < vt1) {
-                a0 += p01[q].x;
-                a1 += p01[q].y;
-                a2 += p23[q].x;
-                a3 += p23[q].y;
-            }
+            const bool in = v0 + q < vt1;  // a select, not a branch, keeps the loads above
+            a0 += in ? p01[q].x : 0.0;
+            a1 += in ? p01[q].y : 0.0;
+            a2 += in ? p23[q].x : 0.0;
+            a3 += in ? p23[q].y : 0.0;
         }
     }
     s[0] = a0;
