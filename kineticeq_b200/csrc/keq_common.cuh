@@ -141,6 +141,16 @@ struct FracMax {
             special = (q != q || special != special) ? q + special : (q > special ? q : special);
         }
     }
+    // The common case of add() without a branch: finite a >= 0 and a finite
+    // positive b.  Returns false (and changes nothing) otherwise; the caller
+    // then redoes its inputs with add(), which is idempotent for a max.
+    __device__ __forceinline__ bool add_normal(double a, double b) {
+        const bool normal = b > 0.0 && b < 1.0e300 && a >= 0.0 && a < 1.0e300;
+        const bool take = normal && (a * den > num * b);
+        num = take ? a : num;
+        den = take ? b : den;
+        return normal;
+    }
     __device__ __forceinline__ double value() const {
         const double q = num / den;
         if (special != special) return special;

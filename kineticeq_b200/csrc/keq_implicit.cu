@@ -325,11 +325,12 @@ __device__ __forceinline__ void stage_coeffs(WarpSmem& w, const TileGeo& g, int 
             // so that each batch is in flight together
             double al[kMaxAACols];
             int col[kMaxAACols];
+            const int col0 = ((head_out - mh) % I.aa_cols + I.aa_cols) % I.aa_cols;
 #pragma unroll
             for (int jj = 0; jj < kMaxAACols; ++jj) {
                 const int jc = jj < mh ? jj : mh - 1;
                 al[jj] = ld_cg(&I.alpha[(size_t)(m - 1) * kMaxAACols + jc]);
-                col[jj] = ((head_out - mh + jc) % I.aa_cols + I.aa_cols) % I.aa_cols;
+                col[jj] = col0 + jc >= I.aa_cols ? col0 + jc - I.aa_cols : col0 + jc;
             }
             double wv[3];
 #pragma unroll
@@ -440,33 +441,53 @@ __device__ bool picard_tile(WarpSmem& w, int vt, int c, int m, unsigned long lon
         ok = lookback(I.agg, I.inc, I.flag, I.nvt, vt, c, epoch, limit, X);
     }
     if (c + 1 < I.nchunks) publish_inc(I.inc, I.flag, tid, fma(P, X, Y), epoch);
-    // recurrence, write, residual
+    // recurrence, write, residual.  The rows of a batch are branch-free
+    // (clamped row index, selects, a predicated store) so that the compiler
+    // can overlap their independent work; the residual takes the select-only
+    // path of FracMax, and a tile that met a non-finite or non-positive ratio
+    // term redoes its residual with the full update afterwards.
     const double tol = I.tol, abs_tol = I.abs_tol;
+    bool odd = false;
 #pragma unroll 1
     for (int r0 = 0; r0 < nr; r0 += 8) {
         double onx[8];
 #pragma unroll
         for (int t = 0; t < 8; ++t) onx[t] = ld_ref(r0 + 8 + t);
+        const int nb = nr - r0;
 #pragma unroll
         for (int t = 0; t < 8; ++t) {
-            const int r = r0 + t;
-            if (r < nr) {
-                const double a = cpl * recip_ge1(one_plus + w.coef[r][3]);
-                X = fma(a, X, w.a[r][lane]);
-                const double x = g.lane_ok ? X : 0.0;
-                w.a[r][lane] = x;
-                if (g.lane_ok) {
-                    const double o = on[t];
-                    const double df = fabs(x - o);
-                    const double ref = nan_max(fabs(x), fabs(o));
-                    q1.add(df, abs_tol + tol * ref);
-                    q2.add(df, (ref != ref || ref >= abs_tol) ? ref : abs_tol);
-                    bad |= !isfinite(x);
-                }
-            }
+            const bool in = t < nb;
+            const int r = in ? r0 + t : r0;
+            const double a = cpl * recip_ge1(one_plus + w.coef[r][3]);
+            const double Xn = fma(a, X, w.a[r][lane]);
+            X = in ? Xn : X;
+            const double x = g.lane_ok ? X : 0.0;
+            if (in) w.a[r][lane] = x;
+            const bool use = in && g.lane_ok;
+            const double o = on[t];
+            const double df = use ? fabs(x - o) : 0.0;
+            const double ref = use ? nan_max(fabs(x), fabs(o)) : 0.0;
+            const double b1 = use ? abs_tol + tol * ref : 1.0;
+            const double b2 = use ? ((ref != ref || ref >= abs_tol) ? ref : abs_tol) : 1.0;
+            const bool n1 = q1.add_normal(df, b1);
+            const bool n2 = q2.add_normal(df, b2);
+            odd |= !(n1 && n2);
+            bad |= use && !isfinite(x);
         }
 #pragma unroll
         for (int t = 0; t < 8; ++t) on[t] = onx[t];
+    }
+    if (__any_sync(0xffffffffu, odd) && g.lane_ok) {
+        // rare: the full residual update over the tile's rows (f^(m) is still
+        // in place; the tile's rows are written after the reduction)
+        for (int r = 0; r < nr; ++r) {
+            const double x = w.a[r][lane];
+            const double o = ld_ref(r);
+            const double df = fabs(x - o);
+            const double ref = nan_max(fabs(x), fabs(o));
+            q1.add(df, abs_tol + tol * ref);
+            q2.add(df, (ref != ref || ref >= abs_tol) ? ref : abs_tol);
+        }
     }
     store_partials(w, g, vt);
     return ok;
