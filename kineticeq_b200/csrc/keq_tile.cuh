@@ -29,7 +29,8 @@ namespace keq {
 
 constexpr int kRmax = 32;   // rows (scan positions) per tile at most
 constexpr int kRB = 32;     // rows per row block (unit of the row reductions)
-constexpr int kWin = 32;    // predecessor chunks polled per look-back round
+constexpr int kWin = 32;    // predecessor chunks polled per look-back round (one per lane)
+constexpr int kWinRounds = 4;  // rounds a look-back may reach back: 128 chunks
 constexpr int kPartQ = 4;   // doubles per (v-tile, row) partial: sum x, x v, x v^2, x v^3
 constexpr unsigned long long kFlagAgg = 1ull, kFlagInc = 2ull;
 
@@ -97,30 +98,43 @@ __device__ __forceinline__ void publish_inc(double* inc, unsigned long long* fla
 }
 
 // Carry into chunk c >= 1 of v-tile column vt (tile index t = chunk * nvt +
-// vt).  Lane q polls chunk c-1-q (relaxed; the fence after the wait makes it
-// an acquire); the nearest chunk with an inclusive value whose successors up
-// to c-1 all have aggregates is the base.  Bounded: on timeout returns false
+// vt).  Round r polls chunks c-1-32r-lane (relaxed; the fence after the wait
+// makes it an acquire); the nearest chunk with an inclusive value whose
+// successors up to c-1 all have aggregates is the base.  A deeper round is
+// polled only when every chunk of the rounds before it has an aggregate but
+// none an inclusive value, so a chunk far from the resolved prefix can start
+// from an inclusive value up to 128 chunks back instead of waiting for the
+// prefix to advance 32 chunks at a time.  Bounded: on timeout returns false
 // (X = 0).
 __device__ __forceinline__ bool lookback(const double* agg, const double* inc,
                                          const unsigned long long* flag, int nvt, int vt, int c,
                                          unsigned long long epoch, unsigned long long limit,
                                          double& X) {
     const int lane = threadIdx.x & 31;
-    const int nval = c < kWin ? c : kWin;
+    const int nval = c < kWin * kWinRounds ? c : kWin * kWinRounds;
     unsigned long long it = 0;
     unsigned ns = 32;
     int q = -1;
     for (;;) {
-        unsigned long long f = 0ull;
-        if (lane < nval) f = ld_relaxed64(&flag[(size_t)(c - 1 - lane) * nvt + vt]);
-        const bool cur = (f >> 2) == epoch;
-        const unsigned incm = __ballot_sync(0xffffffffu, cur && (f & 3ull) == kFlagInc);
-        const unsigned aggm = __ballot_sync(0xffffffffu, cur && (f & 3ull) != 0ull);
-        if (incm != 0u) {
-            q = __ffs(incm) - 1;
-            const unsigned need = (q == 0) ? 0u : ((1u << q) - 1u);
-            if ((aggm & need) == need) break;
+        // every branch below is warp-uniform (ballot results)
+        for (int rd = 0; rd < kWinRounds && rd * kWin < nval; ++rd) {
+            const int qq = rd * kWin + lane;
+            unsigned long long f = 0ull;
+            if (qq < nval) f = ld_relaxed64(&flag[(size_t)(c - 1 - qq) * nvt + vt]);
+            const bool cur = (f >> 2) == epoch;
+            const unsigned incm = __ballot_sync(0xffffffffu, cur && (f & 3ull) == kFlagInc);
+            const unsigned aggm = __ballot_sync(0xffffffffu, cur && (f & 3ull) != 0ull);
+            if (incm != 0u) {
+                const int qr = __ffs(incm) - 1;
+                const unsigned need = (qr == 0) ? 0u : ((1u << qr) - 1u);
+                if ((aggm & need) == need) q = rd * kWin + qr;
+                break;
+            }
+            const int left = nval - rd * kWin;
+            const unsigned valid = left >= 32 ? 0xffffffffu : ((1u << left) - 1u);
+            if ((aggm & valid) != valid) break;  // a missing aggregate: no deeper base
         }
+        if (q >= 0) break;
         if (++it > limit) {
             X = 0.0;
             return false;
