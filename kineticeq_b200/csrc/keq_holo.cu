@@ -1076,22 +1076,30 @@ __device__ __noinline__ bool dist_tile(WarpSmem& w, int vt, int c, int z, unsign
         ok = lookback(I.agg, I.inc, I.flag, I.nvt, vt, c, epoch, limit, X);
     }
     if (c + 1 < I.nchunks) publish_inc(I.inc, I.flag, tid, fma(P, X, Y), epoch);
+    // rows without branches (selects and a predicated store) so that their
+    // independent work overlaps; the residual takes FracMax's select-only path
+    // and a tile that met a non-finite or non-positive term redoes it in full
     const double tol = I.ho_tol, abs_tol = I.ho_abs_tol;
+    bool odd = false;
 #pragma unroll 4
     for (int r = 0; r < nr; ++r) {
         const double a = cpl * recip_ge1(one_plus + w.coef[r][3]);
         X = fma(a, X, w.a[r][lane]);
         const double x = g.lane_ok ? X : 0.0;
         w.a[r][lane] = x;
-        if (g.lane_ok) {
-            fo[(size_t)scan_row(nx, g.pos, g.s0 + r) * nv + g.j] = x;
-            const double o = w.o[r][lane];
-            const double df = fabs(x - o);
-            const double ref = nan_max(fabs(x), fabs(o));
-            q1.add(df, abs_tol + tol * ref);
-            mdf = nan_max(mdf, df);
-            mref = nan_max(mref, ref);
-            bad |= !isfinite(x);
+        if (g.lane_ok) fo[(size_t)scan_row(nx, g.pos, g.s0 + r) * nv + g.j] = x;
+        const double o = w.o[r][lane];
+        const double df = g.lane_ok ? fabs(x - o) : 0.0;
+        const double ref = g.lane_ok ? nan_max(fabs(x), fabs(o)) : 0.0;
+        odd |= !q1.add_normal(df, g.lane_ok ? abs_tol + tol * ref : 1.0);
+        mdf = nan_max(mdf, df);
+        mref = nan_max(mref, ref);
+        bad |= g.lane_ok && !isfinite(x);
+    }
+    if (__any_sync(0xffffffffu, odd) && g.lane_ok) {
+        for (int r = 0; r < nr; ++r) {
+            const double x = w.a[r][lane], o = w.o[r][lane];
+            q1.add(fabs(x - o), abs_tol + tol * nan_max(fabs(x), fabs(o)));
         }
     }
     store_partials_h(w, g, vt);
