@@ -524,12 +524,16 @@ __device__ bool picard_tile32(WarpSmem& w, int vt, int c, int m, unsigned long l
         }
     }
     cp_async_commit();
+    // the previous iterate of every row, loaded unconditionally (rows past the
+    // tile and absent velocities read a clamped, present cell; their values
+    // are selected out) so that the 32 loads are in flight together
     float fbv[kRmax];
+    const int jc = g.j < 0 ? 0 : (g.j >= nv ? nv - 1 : g.j);
 #pragma unroll
-    for (int r = 0; r < kRmax; ++r)
-        fbv[r] = (r < nr && g.lane_ok)
-                     ? __ldcg(&ref[(size_t)scan_row(nx, g.pos, g.s0 + r) * nv + g.j])
-                     : 0.0f;
+    for (int r = 0; r < kRmax; ++r) {
+        const int rc = r < nr ? r : nr - 1;
+        fbv[r] = __ldcg(&ref[(size_t)scan_row(nx, g.pos, g.s0 + rc) * nv + jc]);
+    }
     const double vjd = g.lane_ok ? __ldg(&I.v[g.j]) : 0.0;
     w.vv[lane] = vjd;
     stage_coeffs(w, g, vt, m);
@@ -569,21 +573,35 @@ __device__ bool picard_tile32(WarpSmem& w, int vt, int c, int m, unsigned long l
     __syncwarp();  // every lane has read its f^n (FP32) before the buffer takes x
     float X = (float)Xd;
     const double tol = I.tol32, abs_tol = I.abs_tol;
+    // branch-free rows (selects, a predicated store) with the select-only
+    // residual; a tile that met a non-finite or non-positive term redoes the
+    // residual with the full update
+    bool odd = false;
 #pragma unroll
     for (int r = 0; r < kRmax; ++r) {
-        if (r < nr) {
-            const float a = cpl / (one_plus + (float)w.coef[r][3]);
-            X = fmaf(a, X, cvs[r]);
-            const float x = g.lane_ok ? X : 0.0f;
-            w.a[r][lane] = (double)x;
-            if (g.lane_ok) {
-                const double o = (double)fbv[r];
-                const double df = fabs((double)x - o);
-                const double rf = nan_max(fabs((double)x), fabs(o));
-                q1.add(df, abs_tol + tol * rf);
-                q2.add(df, (rf != rf || rf >= abs_tol) ? rf : abs_tol);
-                bad |= !isfinite(x);
-            }
+        const bool in = r < nr;
+        const float a = cpl / (one_plus + (float)w.coef[r][3]);
+        const float Xn = fmaf(a, X, cvs[r]);
+        X = in ? Xn : X;
+        const float x = g.lane_ok ? X : 0.0f;
+        if (in) w.a[r][lane] = (double)x;
+        const bool use = in && g.lane_ok;
+        const double o = (double)fbv[r];
+        const double df = use ? fabs((double)x - o) : 0.0;
+        const double rf = use ? nan_max(fabs((double)x), fabs(o)) : 0.0;
+        const bool n1 = q1.add_normal(df, use ? abs_tol + tol * rf : 1.0);
+        const bool n2 = q2.add_normal(df, use ? ((rf != rf || rf >= abs_tol) ? rf : abs_tol) : 1.0);
+        odd |= !(n1 && n2);
+        bad |= use && !isfinite(x);
+    }
+    if (__any_sync(0xffffffffu, odd) && g.lane_ok) {
+        for (int r = 0; r < nr; ++r) {
+            const double x = w.a[r][lane];
+            const double o = (double)__ldcg(&ref[(size_t)scan_row(nx, g.pos, g.s0 + r) * nv + g.j]);
+            const double df = fabs(x - o);
+            const double rf = nan_max(fabs(x), fabs(o));
+            q1.add(df, abs_tol + tol * rf);
+            q2.add(df, (rf != rf || rf >= abs_tol) ? rf : abs_tol);
         }
     }
     store_partials(w, g, vt);
