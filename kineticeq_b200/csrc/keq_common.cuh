@@ -20,11 +20,6 @@ constexpr double kInvSqrt2Pi = 0.39894228040143267794;  // 1/sqrt(2 pi), correct
 // a wait run out without hanging anything.
 constexpr unsigned long long kSpinLimit = 1ull << 25;
 
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
 // Polling load without ordering; a wait that ends on it is followed by
 // fence_gpu() (relaxed load + fence = acquire), so each poll costs no L1
 // invalidation.
@@ -34,9 +29,6 @@ __device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
     return v;
 }
 __device__ __forceinline__ void fence_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
-__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
 __device__ __forceinline__ double ld_cg(const double* p) { return __ldcg(p); }
 
 // Non-negative doubles (and +NaN) order like their bit patterns, so the max
@@ -253,23 +245,6 @@ struct PlanHead {
     int trace_iters;
     int fresh;                  // 1 until the first launch completes: stats totals start at 0
 };
-
-// Spin (bounded) until *flag >= want.  Returns false on timeout.
-__device__ __forceinline__ bool wait_flag_geq(const unsigned* flag, unsigned want, int* err,
-                                              unsigned long long limit = kSpinLimit) {
-    unsigned long long it = 0;
-    unsigned ns = 16;
-    while (ld_relaxed(flag) < want) {
-        if (++it > limit) {
-            atomicOr(err, 1 << KEQ_ERR_TIMEOUT);
-            return false;
-        }
-        __nanosleep(ns);
-        if (ns < 128) ns <<= 1;
-    }
-    fence_gpu();
-    return true;
-}
 
 // Warp reduce-scatter of ROWS x Q partial sums held by every lane
 // (acc[r*Q + q]).  On return lanes holding row r (see owner_row()) carry the

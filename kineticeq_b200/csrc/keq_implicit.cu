@@ -628,21 +628,6 @@ __device__ __forceinline__ void write_tile(WarpSmem& w, int vt, int c, double* _
     }
 }
 
-// Element j of a small register array (a select chain, so the array stays
-// in registers), and its assignment.
-__device__ __forceinline__ double pick8(const double* a, int j) {
-    double v = 0.0;
-#pragma unroll
-    for (int k = 0; k < kMaxAACols; ++k)
-        if (k == j) v = a[k];
-    return v;
-}
-__device__ __forceinline__ void set8(double* a, int j, double v) {
-#pragma unroll
-    for (int k = 0; k < kMaxAACols; ++k)
-        if (k == j) a[k] = v;
-}
-
 // ---- Anderson: small symmetric solve (Cholesky, min-norm fall-back) -------
 // torch.linalg.cholesky / cholesky_solve with the lstsq fall-back of
 // bgk1d_aa_cpu.py:93-97; the fall-back here is a Jacobi eigen pseudo-inverse.
